@@ -1,0 +1,793 @@
+// api.cu -- host orchestration and the C ABI of libdrtopk.so.
+//
+// One select = memset of a small control block + the delegate sampler + one
+// cooperative "fused" kernel (first select, filter/concatenation, second
+// select, output).  Stream-ordered, no host synchronisation, graph-capturable.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "../../include/drtopk.h"
+#include "fused.cuh"
+#include "plan.h"
+#include "sampler.cuh"
+
+using namespace drtopk;
+
+namespace drtopk {
+
+// ------------------------------------------------------------ device info
+struct DevInfo {
+  int device = -1;
+  int sms = 0;
+  int occ_fused[4] = {0, 0, 0, 0};
+  size_t occ_fused_smem[4] = {0, 0, 0, 0};
+  int occ_sample = 0;
+};
+
+static std::mutex g_dev_mu;
+static DevInfo g_dev[64];
+
+static cudaError_t dev_info(int device, DevInfo** out) {
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+  DevInfo& d = g_dev[device];
+  if (d.device < 0) {
+    cudaError_t e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return e;
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sample<KM_U32, 2, true>, SAMPLE_THREADS, 0);
+    if (e != cudaSuccess) return e;
+    d.occ_sample = std::max(1, occ);
+    d.device = device;
+  }
+  *out = &d;
+  return cudaSuccess;
+}
+
+template <int KM>
+static void* fused_fn() {
+  return (void*)k_fused<KM>;
+}
+static void* fused_ptr(int km) {
+  switch (km) {
+    case KM_U32: return fused_fn<KM_U32>();
+    case KM_F32: return fused_fn<KM_F32>();
+    case KM_U32_MIN: return fused_fn<KM_U32_MIN>();
+    default: return fused_fn<KM_F32_MIN>();
+  }
+}
+
+static cudaError_t fused_max_grid(DevInfo* d, int km, size_t smem, int* grid) {
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  if (d->occ_fused[km] == 0 || d->occ_fused_smem[km] != smem) {
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_ptr(km), FUSED_THREADS, smem);
+    if (e != cudaSuccess) return e;
+    d->occ_fused[km] = std::max(1, occ);
+    d->occ_fused_smem[km] = smem;
+  }
+  *grid = d->occ_fused[km] * d->sms;
+  return cudaSuccess;
+}
+
+// ------------------------------------------------------------ planning
+static inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+int ref_alpha(double log2n, double k) {
+  // baseline+filter+beta+shuffle/main.cu:83, evaluated as the reference does
+  return (int)(0.5 * (log2n - std::log(k) / std::log(2.0) + 3));
+}
+
+drtopk_status_t make_plan(uint64_t n, uint64_t k, drtopk_dtype_t dtype, const drtopk_params_t* pin, int sms,
+                          int fused_grid, Plan* P) {
+  drtopk_params_t p;
+  if (pin) p = *pin;
+  else drtopk_params_default(&p);
+  std::memset(P, 0, sizeof(*P));
+  if (n == 0 || k < 1 || k > n) return DRTOPK_EINVAL;
+  if (n > 0xffffffffull) return DRTOPK_EUNSUPPORTED;
+  if (dtype != DRTOPK_U32 && dtype != DRTOPK_F32) return DRTOPK_EINVAL;
+  if (!(p.nbits == 1 || p.nbits == 2 || p.nbits == 4 || p.nbits == 8)) return DRTOPK_EINVAL;
+  if (p.algo == DRTOPK_ALGO_AUTO || p.alpha == -2) {
+    drtopk_status_t s = drtopk_autotune(n, k, dtype, &p);
+    if (s != DRTOPK_OK) return s;
+  }
+  if (p.algo != DRTOPK_ALGO_RADIX && p.algo != DRTOPK_ALGO_BUCKET && p.algo != DRTOPK_ALGO_PLAIN_RADIX)
+    return DRTOPK_EUNSUPPORTED;  // bitonic has its own entry point
+  P->n = n;
+  P->k = k;
+  P->km = (dtype == DRTOPK_F32 ? 1 : 0) + (p.largest ? 0 : 2);
+  P->algo = p.algo;
+  P->bucket = p.algo == DRTOPK_ALGO_BUCKET;
+  P->nbits = p.nbits;
+  if (P->bucket) {
+    if (p.num_bucket < 2 || p.num_bucket > 4096) return DRTOPK_EINVAL;
+    P->nb = p.num_bucket;
+  } else {
+    P->nb = 1 << p.nbits;
+  }
+  P->sorted = p.sorted;
+  const double log2n = std::log2((double)n);
+  int alpha = p.alpha;
+  const bool auto_alpha = alpha < 0;
+  if (auto_alpha) {
+    alpha = ref_alpha(log2n, (double)k);
+    if (P->bucket && alpha < 5) alpha++;  // bucket_select/main.cu:67
+  }
+  if (alpha > 24) return DRTOPK_EINVAL;
+  if (p.algo == DRTOPK_ALGO_PLAIN_RADIX || alpha <= 0) {
+    P->path = PATH_PLAIN;
+    P->alpha = 0;
+  } else {
+    int path;
+    if (p.path == 0) path = alpha > 5 ? PATH_DEFAULT : PATH_BETA;  // main.cu:87-89
+    else if (p.path == 1) path = PATH_DEFAULT;
+    else if (p.path == 2) path = PATH_BETA;
+    else return DRTOPK_EINVAL;
+    if (path == PATH_BETA && p.beta != 2) return DRTOPK_EINVAL;  // beta 3/4 paths are broken in the reference
+    uint64_t S = 1ull << alpha;
+    uint64_t M = (n + S - 1) >> alpha;
+    if (path == PATH_DEFAULT) {
+      if (M < k || alpha < 2) {
+        if (!auto_alpha || p.path == 1) return DRTOPK_EINVAL;
+        // non-power-of-two n: shrink the subranges until k fit, else beta path
+        while (alpha > 5 && ((n + (1ull << alpha) - 1) >> alpha) < k) alpha--;
+        if (alpha <= 5) path = PATH_BETA;
+        S = 1ull << alpha;
+        M = (n + S - 1) >> alpha;
+      }
+    }
+    if (path == PATH_BETA && alpha > 16) return DRTOPK_EINVAL;
+    P->path = path;
+    P->alpha = alpha;
+    P->S = S;
+    P->M = M;
+  }
+  const int D = 32 / P->nbits;
+  if (P->path == PATH_BETA) {
+    if (P->bucket) P->first_levels = 2;  // bucketselect_combined.cuh:972-1095 (two bucket levels)
+    else P->first_levels = p.first_digits > 0 ? std::min(p.first_digits, D) : std::max(0, D - 3);
+  }
+  P->fused_grid = fused_grid;
+  return DRTOPK_OK;
+}
+
+// workspace layout; want_idx decides whether the beta sampler records positions
+void layout(Plan* P, bool want_idx) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += align256(bytes);
+    return o;
+  };
+  const uint64_t k = P->k;
+  P->has_pos = (P->path == PATH_BETA && want_idx) ? 1 : 0;
+  // control block (zeroed each call)
+  P->run_words = 3 * P->nb + (MAX_LEVELS + 2) + 1;
+  size_t ctrl_words = CTRL_HDR_WORDS + 4 * (size_t)P->run_words + 8 * 256;
+  P->off_ctrl = take(ctrl_words * 4);
+  P->ctrl_bytes = ctrl_words * 4;
+  uint64_t ncand_cap = 0;
+  if (P->path == PATH_DEFAULT) {
+    P->off_del = take(P->M * 4);
+    P->off_Atop = take(k * 8);
+    P->off_Acbuf0 = take(P->M * 8);
+    P->off_Acbuf1 = take(P->M * 8);
+    ncand_cap = std::min<uint64_t>(P->n, k * P->S);
+  } else if (P->path == PATH_BETA) {
+    P->off_del = take(P->M * 8);
+    if (P->has_pos) P->off_pos = take(P->M * 2);
+    ncand_cap = P->n;
+  } else {
+    ncand_cap = P->n;
+  }
+  P->cand_cap = ncand_cap;
+  P->off_cand = take(ncand_cap * 8);
+  P->off_Ccbuf0 = take(ncand_cap * 8);
+  P->off_Ctop = take(k * 8);
+  if (P->sorted && k > (uint64_t)SMALL_SORT) {
+    P->off_sort0 = take(k * 8);
+    P->off_sort1 = take(k * 8);
+    P->off_sortcnt = take((size_t)P->fused_grid * 256 * 4);
+  }
+  P->ws_bytes = off;
+}
+
+}  // namespace drtopk
+
+// ------------------------------------------------------------ handle
+struct drtopk_handle {
+  int device = 0;
+  size_t budget = 0;
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  void* last_ctrl = nullptr;  // control block of the last call (for stats)
+  Plan last_plan;
+  bool have_last = false;
+  std::vector<cudaEvent_t> prof;  // 3 events per recorded call
+  int prof_max = 0, prof_used = 0;
+  bool prof_on = false;
+  std::mutex mu;
+};
+
+extern "C" void drtopk_params_default(drtopk_params_t* p) {
+  p->nbits = 8;
+  p->alpha = -1;
+  p->beta = 2;
+  p->path = 0;
+  p->algo = DRTOPK_ALGO_RADIX;
+  p->num_bucket = 256;
+  p->largest = 1;
+  p->sorted = 0;
+  p->first_digits = 0;
+}
+
+extern "C" const char* drtopk_status_str(drtopk_status_t s) {
+  switch (s) {
+    case DRTOPK_OK: return "ok";
+    case DRTOPK_EINVAL: return "invalid argument";
+    case DRTOPK_ENOMEM: return "out of device memory / workspace too small";
+    case DRTOPK_ECUDA: return "CUDA error";
+    case DRTOPK_EDEVICE: return "device-side check failed";
+    case DRTOPK_EBUDGET: return "HBM budget exceeded";
+    case DRTOPK_EUNSUPPORTED: return "unsupported";
+    case DRTOPK_ETIMEOUT: return "device wait timed out";
+    case DRTOPK_EAGAIN: return "try again";
+    case DRTOPK_ECANCELLED: return "cancelled";
+  }
+  return "unknown";
+}
+
+extern "C" drtopk_status_t drtopk_create(drtopk_handle_t* h, int device, size_t hbm_budget_bytes) {
+  if (!h) return DRTOPK_EINVAL;
+  *h = nullptr;
+  int cur = 0;
+  if (cudaGetDevice(&cur) != cudaSuccess) return DRTOPK_ECUDA;
+  if (cudaSetDevice(device) != cudaSuccess) return DRTOPK_EINVAL;
+  DevInfo* di = nullptr;
+  if (dev_info(device, &di) != cudaSuccess) { cudaSetDevice(cur); return DRTOPK_ECUDA; }
+  drtopk_handle* hh = new (std::nothrow) drtopk_handle();
+  if (!hh) { cudaSetDevice(cur); return DRTOPK_ENOMEM; }
+  hh->device = device;
+  hh->budget = hbm_budget_bytes;
+  for (auto& e : hh->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) { cudaSetDevice(cur); delete hh; return DRTOPK_ECUDA; }
+  cudaSetDevice(cur);
+  *h = hh;
+  return DRTOPK_OK;
+}
+
+extern "C" drtopk_status_t drtopk_destroy(drtopk_handle_t h) {
+  if (!h) return DRTOPK_OK;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(h->device);
+  if (h->ws) cudaFree(h->ws);
+  for (auto& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : h->prof)
+    if (e) cudaEventDestroy(e);
+  cudaSetDevice(cur);
+  delete h;
+  return DRTOPK_OK;
+}
+
+static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype_t dtype, const drtopk_params_t* p,
+                                bool want_idx, Plan* P, DevInfo** dout) {
+  DevInfo* di = nullptr;
+  if (dev_info(device, &di) != cudaSuccess) return DRTOPK_ECUDA;
+  drtopk_status_t s = make_plan(n, k, dtype, p, di->sms, 0, P);
+  if (s != DRTOPK_OK) return s;
+  // dynamic shared memory of the fused kernel
+  size_t smem = (size_t)std::max(P->nb, 256) * 4;
+  if (P->sorted && k <= (uint64_t)SMALL_SORT) {
+    size_t np2 = 1;
+    while (np2 < k) np2 <<= 1;
+    smem = std::max(smem, np2 * 8);
+  }
+  P->fused_smem = smem;
+  int maxgrid = 0;
+  if (fused_max_grid(di, P->km, smem, &maxgrid) != cudaSuccess) return DRTOPK_ECUDA;
+  // grid: the whole GPU for large inputs, fewer CTAs for small ones (fewer
+  // barrier participants)
+  uint64_t want = std::max<uint64_t>((uint64_t)di->sms / 2, n >> 15);
+  P->fused_grid = (int)std::min<uint64_t>((uint64_t)maxgrid, std::max<uint64_t>(1, want));
+  // sampler grid: persistent, capped by the work items
+  if (P->path != PATH_PLAIN) {
+    uint64_t items = P->alpha >= 9 ? P->M : ((n + 511) >> 9);
+    uint64_t ctas = (items + SAMPLE_WARPS - 1) / SAMPLE_WARPS;
+    P->sample_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(ctas, (uint64_t)di->sms * di->occ_sample));
+  }
+  layout(P, want_idx);
+  if (dout) *dout = di;
+  return DRTOPK_OK;
+}
+
+extern "C" drtopk_status_t drtopk_workspace_size(uint64_t n, uint64_t k, drtopk_dtype_t dtype,
+                                                 const drtopk_params_t* p, size_t* bytes) {
+  if (!bytes) return DRTOPK_EINVAL;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    // no device: plan with a nominal B200 shape (148 SMs, 4 CTAs/SM)
+    Plan P;
+    drtopk_status_t s = make_plan(n, k, dtype, p, 148, 592, &P);
+    if (s != DRTOPK_OK) return s;
+    layout(&P, true);
+    *bytes = P.ws_bytes;
+    return DRTOPK_OK;
+  }
+  Plan P;
+  drtopk_status_t s = plan_for(dev, n, k, dtype, p, true, &P, nullptr);
+  if (s != DRTOPK_OK) {
+    // CPU-only process or unusable device: fall back to the nominal shape
+    if (s != DRTOPK_ECUDA) return s;
+    s = make_plan(n, k, dtype, p, 148, 592, &P);
+    if (s != DRTOPK_OK) return s;
+    layout(&P, true);
+  }
+  *bytes = P.ws_bytes;
+  return DRTOPK_OK;
+}
+
+// ------------------------------------------------------------ launch
+namespace drtopk {
+
+template <int KM>
+static cudaError_t launch_sample(const SampleArgs& sa, int beta, bool pos, int grid, cudaStream_t st) {
+  if (beta == 2) {
+    if (pos) k_sample<KM, 2, true><<<grid, SAMPLE_THREADS, 0, st>>>(sa);
+    else k_sample<KM, 2, false><<<grid, SAMPLE_THREADS, 0, st>>>(sa);
+  } else {
+    k_sample<KM, 1, false><<<grid, SAMPLE_THREADS, 0, st>>>(sa);
+  }
+  return cudaGetLastError();
+}
+
+static RunBufs run_bufs(char* ctrl, const Plan& P, int which) {
+  uint32_t* base = reinterpret_cast<uint32_t*>(ctrl) + CTRL_HDR_WORDS + (size_t)which * P.run_words;
+  RunBufs r;
+  r.H[0] = base;
+  r.H[1] = base + P.nb;
+  r.H[2] = base + 2 * P.nb;
+  r.set_count = base + 3 * P.nb;
+  r.top_count = base + 3 * P.nb + MAX_LEVELS + 2;
+  r.cbuf[0] = r.cbuf[1] = nullptr;
+  r.top = nullptr;
+  return r;
+}
+
+drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, void* d_kth, void* d_vals,
+                               int64_t* d_idx, char* ws, cudaStream_t st, cudaEvent_t* ev) {
+  char* ctrl = ws + P.off_ctrl;
+  uint32_t* cw = reinterpret_cast<uint32_t*>(ctrl);
+  if (cudaMemsetAsync(ctrl, 0, P.ctrl_bytes, st) != cudaSuccess) return DRTOPK_ECUDA;
+  if (ev) cudaEventRecord(ev[0], st);
+  const bool vec_ok = (reinterpret_cast<uintptr_t>(d_keys) & 15u) == 0;
+  FusedArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.keys = static_cast<const uint32_t*>(d_keys);
+  a.n = P.n;
+  a.k = (uint32_t)P.k;
+  a.km = P.km;
+  a.path = P.path;
+  a.bucket = P.bucket;
+  a.nbits = P.nbits;
+  a.nb = P.nb;
+  a.alpha = P.alpha;
+  a.M = P.M;
+  a.first_levels = P.first_levels;
+  a.vec_ok = vec_ok;
+  a.del_minmax = cw + CW_DEL_MINMAX;
+  a.A = run_bufs(ctrl, P, 0);
+  a.AF = run_bufs(ctrl, P, 1);
+  a.C = run_bufs(ctrl, P, 2);
+  a.CF = run_bufs(ctrl, P, 3);
+  a.cand_count = cw + CW_CAND_COUNT;
+  a.cand_minmax = cw + CW_CAND_MINMAX;
+  a.stats = cw + CW_STATS;
+  a.sort_tot = cw + CTRL_HDR_WORDS + 4 * (size_t)P.run_words;
+  a.gb.count = cw + CW_BAR_COUNT;
+  a.gb.gen = cw + CW_BAR_GEN;
+  a.gb.err = cw + CW_ERR;
+  a.gb.nblocks = (uint32_t)P.fused_grid;
+  a.out_kth = static_cast<uint32_t*>(d_kth);
+  a.out_vals = static_cast<uint32_t*>(d_vals);
+  a.out_idx = d_idx;
+  a.sorted = P.sorted;
+  a.cand = reinterpret_cast<uint2*>(ws + P.off_cand);
+  a.cand_cap = P.cand_cap;
+  a.C.top = reinterpret_cast<uint2*>(ws + P.off_Ctop);
+  a.C.cbuf[0] = reinterpret_cast<uint2*>(ws + P.off_Ccbuf0);
+  a.C.cbuf[1] = a.cand;  // level >= 1 may overwrite the candidates
+  if (P.path == PATH_DEFAULT) {
+    a.del = reinterpret_cast<const uint32_t*>(ws + P.off_del);
+    a.A.top = reinterpret_cast<uint2*>(ws + P.off_Atop);
+    a.A.cbuf[0] = reinterpret_cast<uint2*>(ws + P.off_Acbuf0);
+    a.A.cbuf[1] = reinterpret_cast<uint2*>(ws + P.off_Acbuf1);
+  } else if (P.path == PATH_BETA) {
+    a.del = reinterpret_cast<const uint32_t*>(ws + P.off_del);
+    a.has_pos = P.has_pos;
+    if (P.has_pos) a.pos = reinterpret_cast<const uint16_t*>(ws + P.off_pos);
+  }
+  if (P.sorted && P.k > (uint64_t)SMALL_SORT) {
+    a.sort_buf[0] = reinterpret_cast<uint64_t*>(ws + P.off_sort0);
+    a.sort_buf[1] = reinterpret_cast<uint64_t*>(ws + P.off_sort1);
+    a.sort_cnt = reinterpret_cast<uint32_t*>(ws + P.off_sortcnt);
+  }
+  // ---- sampler
+  if (P.path != PATH_PLAIN) {
+    SampleArgs sa;
+    sa.keys = a.keys;
+    sa.n = P.n;
+    sa.alpha = P.alpha;
+    sa.nbits = P.nbits;
+    sa.hmode = P.bucket ? 2 : 1;
+    sa.vec_ok = vec_ok;
+    sa.del = const_cast<uint32_t*>(a.del);
+    sa.pos = const_cast<uint16_t*>(a.pos);
+    sa.hist = a.A.H[0];
+    sa.minmax = cw + CW_DEL_MINMAX;
+    const int beta = P.path == PATH_BETA ? 2 : 1;
+    cudaError_t e;
+    switch (P.km) {
+      case KM_U32: e = launch_sample<KM_U32>(sa, beta, P.has_pos, P.sample_grid, st); break;
+      case KM_F32: e = launch_sample<KM_F32>(sa, beta, P.has_pos, P.sample_grid, st); break;
+      case KM_U32_MIN: e = launch_sample<KM_U32_MIN>(sa, beta, P.has_pos, P.sample_grid, st); break;
+      default: e = launch_sample<KM_F32_MIN>(sa, beta, P.has_pos, P.sample_grid, st); break;
+    }
+    if (e != cudaSuccess) return DRTOPK_ECUDA;
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  // ---- fused cooperative kernel
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P.fused_grid);
+  cfg.blockDim = dim3(FUSED_THREADS);
+  cfg.dynamicSmemBytes = P.fused_smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* args[] = {&a};
+  if (cudaLaunchKernelExC(&cfg, fused_ptr(P.km), args) != cudaSuccess) return DRTOPK_ECUDA;
+  if (ev) cudaEventRecord(ev[2], st);
+  return DRTOPK_OK;
+}
+
+}  // namespace drtopk
+
+static drtopk_status_t ensure_ws(drtopk_handle_t h, size_t bytes) {
+  if (h->ws_bytes >= bytes) return DRTOPK_OK;
+  if (h->budget && bytes > h->budget) return DRTOPK_EBUDGET;
+  if (h->ws) {
+    cudaFree(h->ws);
+    h->ws = nullptr;
+    h->ws_bytes = 0;
+  }
+  size_t want = std::max(bytes, (size_t)(1 << 20));
+  if (cudaMalloc(&h->ws, want) != cudaSuccess) {
+    cudaGetLastError();
+    return DRTOPK_ENOMEM;
+  }
+  h->ws_bytes = want;
+  return DRTOPK_OK;
+}
+
+static drtopk_status_t select_impl(drtopk_handle_t h, const void* d_keys, drtopk_dtype_t dtype, uint64_t n,
+                                   uint64_t k, const drtopk_params_t* p, void* d_kth, void* d_vals, int64_t* d_idx,
+                                   void* d_ws, size_t ws_bytes, void* stream) {
+  if (!h || !d_keys) return DRTOPK_EINVAL;
+  std::lock_guard<std::mutex> lk(h->mu);
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != h->device) cudaSetDevice(h->device);
+  Plan P;
+  drtopk_status_t s = plan_for(h->device, n, k, dtype, p, d_idx != nullptr, &P, nullptr);
+  char* ws = nullptr;
+  if (s == DRTOPK_OK) {
+    if (d_ws) {
+      if (ws_bytes < P.ws_bytes || (reinterpret_cast<uintptr_t>(d_ws) & 255u)) s = DRTOPK_ENOMEM;
+      ws = static_cast<char*>(d_ws);
+    } else {
+      s = ensure_ws(h, P.ws_bytes);
+      ws = static_cast<char*>(h->ws);
+    }
+  }
+  if (s == DRTOPK_OK) {
+    cudaEvent_t* ev = h->ev;
+    if (h->prof_on && h->prof_used < h->prof_max) ev = &h->prof[3 * (size_t)h->prof_used++];
+    s = enqueue_select(P, h->device, d_keys, d_kth, d_vals, d_idx, ws, static_cast<cudaStream_t>(stream), ev);
+    if (s == DRTOPK_OK) {
+      h->last_ctrl = ws + P.off_ctrl;
+      h->last_plan = P;
+      h->have_last = true;
+    }
+  }
+  if (cur != h->device) cudaSetDevice(cur);
+  return s;
+}
+
+extern "C" drtopk_status_t drtopk_select(drtopk_handle_t h, const void* d_keys, drtopk_dtype_t dtype, uint64_t n,
+                                         uint64_t k, const drtopk_params_t* p, void* d_kth, void* d_vals,
+                                         int64_t* d_idx, void* stream) {
+  return select_impl(h, d_keys, dtype, n, k, p, d_kth, d_vals, d_idx, nullptr, 0, stream);
+}
+
+extern "C" drtopk_status_t drtopk_select_ws(drtopk_handle_t h, const void* d_keys, drtopk_dtype_t dtype, uint64_t n,
+                                            uint64_t k, const drtopk_params_t* p, void* d_kth, void* d_vals,
+                                            int64_t* d_idx, void* d_workspace, size_t workspace_bytes,
+                                            void* stream) {
+  if (!d_workspace) return DRTOPK_EINVAL;
+  return select_impl(h, d_keys, dtype, n, k, p, d_kth, d_vals, d_idx, d_workspace, workspace_bytes, stream);
+}
+
+static drtopk_status_t read_ctrl(drtopk_handle_t h, uint32_t* hdr) {
+  if (!h->have_last) return DRTOPK_EINVAL;
+  if (cudaMemcpy(hdr, h->last_ctrl, CTRL_HDR_WORDS * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return DRTOPK_ECUDA;
+  return DRTOPK_OK;
+}
+
+extern "C" drtopk_status_t drtopk_sync_check(drtopk_handle_t h, void* stream) {
+  if (!h) return DRTOPK_EINVAL;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(h->device);
+  drtopk_status_t s = DRTOPK_OK;
+  if (cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) != cudaSuccess) s = DRTOPK_ECUDA;
+  if (s == DRTOPK_OK && h->have_last) {
+    uint32_t hdr[CTRL_HDR_WORDS];
+    s = read_ctrl(h, hdr);
+    if (s == DRTOPK_OK && hdr[CW_ERR]) s = (hdr[CW_ERR] & DE_BARRIER_TIMEOUT) ? DRTOPK_ETIMEOUT : DRTOPK_EDEVICE;
+  }
+  cudaSetDevice(cur);
+  return s;
+}
+
+extern "C" drtopk_status_t drtopk_last_stats(drtopk_handle_t h, drtopk_stats_t* st) {
+  if (!h || !st) return DRTOPK_EINVAL;
+  std::memset(st, 0, sizeof(*st));
+  if (!h->have_last) return DRTOPK_EINVAL;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(h->device);
+  cudaEventSynchronize(h->ev[2]);
+  uint32_t hdr[CTRL_HDR_WORDS];
+  drtopk_status_t s = read_ctrl(h, hdr);
+  if (s == DRTOPK_OK) {
+    const Plan& P = h->last_plan;
+    const uint32_t* S = hdr + CW_STATS;
+    st->alpha = P.alpha;
+    st->beta = P.path == PATH_BETA ? 2 : (P.path == PATH_DEFAULT ? 1 : 0);
+    st->algo = P.algo;
+    st->first_threshold = S[ST_THR1];
+    st->n_subranges = P.M;
+    st->n_selected = S[ST_NSEL];
+    st->n_lonely = S[ST_NLONELY];
+    st->n_candidates = S[ST_NCAND];
+    st->levels_first = (int)S[ST_LVA];
+    st->levels_second = (int)S[ST_LVC];
+    st->device_error = hdr[CW_ERR];
+    auto t64 = [&](int slot) { return (uint64_t)S[slot] | ((uint64_t)S[slot + 1] << 32); };
+    const uint64_t t0 = t64(ST_T0), t1 = t64(ST_T1), t2 = t64(ST_T2), t3 = t64(ST_T3);
+    float ms_s = 0, ms_all = 0;
+    cudaEventElapsedTime(&ms_s, h->ev[0], h->ev[1]);
+    cudaEventElapsedTime(&ms_all, h->ev[0], h->ev[2]);
+    st->ms_sample = ms_s;
+    st->ms_first = t1 > t0 ? (t1 - t0) * 1e-6 : 0.0;
+    st->ms_concat = t2 > t1 ? (t2 - t1) * 1e-6 : 0.0;
+    st->ms_second = t3 > t2 ? (t3 - t2) * 1e-6 : 0.0;
+    st->ms_total = ms_all;
+  }
+  cudaSetDevice(cur);
+  return s;
+}
+
+extern "C" drtopk_status_t drtopk_profile_begin(drtopk_handle_t h, int max_calls) {
+  if (!h || max_calls < 1) return DRTOPK_EINVAL;
+  std::lock_guard<std::mutex> lk(h->mu);
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(h->device);
+  drtopk_status_t s = DRTOPK_OK;
+  while ((int)h->prof.size() < 3 * max_calls) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) { s = DRTOPK_ECUDA; break; }
+    h->prof.push_back(e);
+  }
+  cudaSetDevice(cur);
+  if (s != DRTOPK_OK) return s;
+  h->prof_max = max_calls;
+  h->prof_used = 0;
+  h->prof_on = true;
+  return DRTOPK_OK;
+}
+
+extern "C" drtopk_status_t drtopk_profile_end(drtopk_handle_t h, double* ms_sample, double* ms_fused, int* ncalls) {
+  if (!h) return DRTOPK_EINVAL;
+  std::lock_guard<std::mutex> lk(h->mu);
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(h->device);
+  double a = 0, b = 0;
+  drtopk_status_t s = DRTOPK_OK;
+  for (int i = 0; i < h->prof_used; ++i) {
+    cudaEvent_t* e = &h->prof[3 * (size_t)i];
+    float x = 0, y = 0;
+    if (cudaEventSynchronize(e[2]) != cudaSuccess) { s = DRTOPK_ECUDA; break; }
+    cudaEventElapsedTime(&x, e[0], e[1]);
+    cudaEventElapsedTime(&y, e[1], e[2]);
+    a += x;
+    b += y;
+  }
+  cudaSetDevice(cur);
+  if (ms_sample) *ms_sample = a;
+  if (ms_fused) *ms_fused = b;
+  if (ncalls) *ncalls = h->prof_used;
+  h->prof_on = false;
+  h->prof_used = 0;
+  return s;
+}
+
+extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_t dtype, drtopk_params_t* p) {
+  if (!p || n == 0 || k < 1 || k > n) return DRTOPK_EINVAL;
+  (void)dtype;
+  // Traffic model of the delegate path (bytes beyond the 4n streaming read):
+  //   one delegate per subrange: ~8n/S (write + first-select read) + 4kS
+  //   (the k kept subranges are re-read) -> minimum near S = sqrt(2n/k).
+  // Small segments (n <= 2^16) are cheaper as a plain select.
+  if (p->algo == DRTOPK_ALGO_AUTO) p->algo = DRTOPK_ALGO_RADIX;
+  if (p->algo == DRTOPK_ALGO_BITONIC) return DRTOPK_OK;
+  if (n <= (1ull << 16) && p->algo == DRTOPK_ALGO_RADIX) {
+    p->algo = DRTOPK_ALGO_PLAIN_RADIX;
+    p->alpha = 0;
+    return DRTOPK_OK;
+  }
+  double s = std::sqrt(2.0 * (double)n / (double)k);
+  int alpha = (int)std::lround(std::log2(std::max(1.0, s)));
+  // keep enough subranges (M >= 8k) so the first select has room to filter
+  while (alpha > 2 && ((n >> alpha) < 8 * k)) alpha--;
+  alpha = std::max(2, std::min(alpha, 16));
+  if (alpha >= 6 && (n >> alpha) >= k) {
+    p->alpha = alpha;
+    p->path = 1;
+  } else {
+    // large k relative to n: two delegates per subrange (beta path) with
+    // small subranges and a two-digit threshold (fewer lonely candidates)
+    alpha = std::max(2, std::min(5, alpha));
+    p->alpha = alpha;
+    p->path = 2;
+    p->beta = 2;
+    if (p->nbits == 8 && p->first_digits == 0) p->first_digits = 2;
+  }
+  return DRTOPK_OK;
+}
+
+// ------------------------------------------------------------ reference-compatible entry points
+static std::mutex g_default_mu;
+static drtopk_handle_t g_default[64];
+
+static drtopk_status_t default_handle(drtopk_handle_t* out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DRTOPK_ECUDA;
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  if (dev < 0 || dev >= 64) return DRTOPK_EINVAL;
+  if (!g_default[dev]) {
+    drtopk_status_t s = drtopk_create(&g_default[dev], dev, 0);
+    if (s != DRTOPK_OK) return s;
+  }
+  *out = g_default[dev];
+  return DRTOPK_OK;
+}
+
+static drtopk_status_t blocking_select(const uint32_t* vec_d, uint64_t n, uint64_t k, const drtopk_params_t* p,
+                                       uint32_t* TopKElement, drtopk_stats_t* st) {
+  drtopk_handle_t h;
+  drtopk_status_t s = default_handle(&h);
+  if (s != DRTOPK_OK) return s;
+  uint32_t* d_kth = nullptr;
+  if (cudaMalloc(&d_kth, 4) != cudaSuccess) return DRTOPK_ENOMEM;
+  s = drtopk_select(h, vec_d, DRTOPK_U32, n, k, p, d_kth, nullptr, nullptr, nullptr);
+  if (s == DRTOPK_OK) s = drtopk_sync_check(h, nullptr);
+  if (s == DRTOPK_OK && cudaMemcpy(TopKElement, d_kth, 4, cudaMemcpyDeviceToHost) != cudaSuccess) s = DRTOPK_ECUDA;
+  if (s == DRTOPK_OK && st) s = drtopk_last_stats(h, st);
+  cudaFree(d_kth);
+  return s;
+}
+
+extern "C" drtopk_status_t drtopk_sample_radix_select(
+    uint32_t* vec_d, int num_element, int k, int num_bucket, uint32_t* TopKElement, int NBitsperDigit,
+    int CurrentDigit, int NSubranges, int SubRangesize, int alpha, double* timeforMaxsample,
+    double* timeforFirstTopK, double* timeForsecondTopK, double* timeforConcatenation, uint32_t* Max_d,
+    int* SubrangeId_d, int NSharedMemoryElements, int SizeOfSubWarp, int pow_size_Subwarp, int NSubWarps_InBlock,
+    int NSubRangesPerBlock, int NElementsPerBlock_ReadFromGlobal, int TotalBlocksrequired, int SizeOfAllocation,
+    int NThreadsPerBlock, int beta, int defaultContribution, int NthreadstoworkInreduction,
+    int* SelectedSubrangeId_d, int* CountLonelyElements_d, int* write_pos_d, uint32_t* ConcatenatedRange_d,
+    int* CountSelectedSubrange_d) {
+  (void)CurrentDigit; (void)SubrangeId_d; (void)NSharedMemoryElements; (void)SizeOfSubWarp;
+  (void)pow_size_Subwarp; (void)NSubWarps_InBlock; (void)NSubRangesPerBlock; (void)NElementsPerBlock_ReadFromGlobal;
+  (void)TotalBlocksrequired; (void)SizeOfAllocation; (void)NThreadsPerBlock; (void)NthreadstoworkInreduction;
+  (void)SelectedSubrangeId_d; (void)ConcatenatedRange_d;
+  if (!vec_d || !TopKElement || num_element <= 0 || k <= 0 || k > num_element) return DRTOPK_EINVAL;
+  if (num_bucket != (1 << NBitsperDigit)) return DRTOPK_EINVAL;
+  if (SubRangesize != (1 << alpha) || NSubranges != num_element / SubRangesize) return DRTOPK_EINVAL;
+  drtopk_params_t p;
+  drtopk_params_default(&p);
+  p.nbits = NBitsperDigit;
+  p.alpha = alpha;
+  p.beta = beta;
+  p.path = defaultContribution ? 1 : 2;
+  drtopk_stats_t st;
+  drtopk_status_t s = blocking_select(vec_d, (uint64_t)num_element, (uint64_t)k, &p, TopKElement, &st);
+  if (s != DRTOPK_OK) return s;
+  if (timeforMaxsample) *timeforMaxsample = st.ms_sample * 1e-3;
+  if (timeforFirstTopK) *timeforFirstTopK = st.ms_first * 1e-3;
+  if (timeforConcatenation) *timeforConcatenation = st.ms_concat * 1e-3;
+  if (timeForsecondTopK) *timeForsecondTopK = st.ms_second * 1e-3;
+  // the reference's observable counters
+  int cnt[3] = {(int)st.n_selected, (int)st.n_lonely, (int)st.n_candidates};
+  if (CountSelectedSubrange_d) cudaMemcpy(CountSelectedSubrange_d, &cnt[0], 4, cudaMemcpyHostToDevice);
+  if (CountLonelyElements_d) cudaMemcpy(CountLonelyElements_d, &cnt[1], 4, cudaMemcpyHostToDevice);
+  if (write_pos_d) cudaMemcpy(write_pos_d, &cnt[2], 4, cudaMemcpyHostToDevice);
+  // the delegates in the caller's Max_d (the reference leaves them there)
+  drtopk_handle_t h;
+  if (Max_d && default_handle(&h) == DRTOPK_OK && h->have_last && h->last_plan.path != PATH_PLAIN) {
+    const Plan& P = h->last_plan;
+    size_t bytes = P.M * (P.path == PATH_BETA ? 8 : 4);
+    cudaMemcpy(Max_d, static_cast<char*>(h->ws) + P.off_del, bytes, cudaMemcpyDeviceToDevice);
+  }
+  return DRTOPK_OK;
+}
+
+extern "C" drtopk_status_t drtopk_radix_select(uint32_t* vec_d, int num_element, int k, int num_bucket,
+                                               uint32_t* TopKElement, int NBitsperDigit, int CurrentDigit) {
+  (void)CurrentDigit;
+  if (!vec_d || !TopKElement || num_element <= 0 || k <= 0 || k > num_element) return DRTOPK_EINVAL;
+  if (num_bucket != (1 << NBitsperDigit)) return DRTOPK_EINVAL;
+  drtopk_params_t p;
+  drtopk_params_default(&p);
+  p.nbits = NBitsperDigit;
+  p.algo = DRTOPK_ALGO_PLAIN_RADIX;
+  return blocking_select(vec_d, (uint64_t)num_element, (uint64_t)k, &p, TopKElement, nullptr);
+}
+
+extern "C" drtopk_status_t drtopk_sample_bucket_select(
+    uint32_t* vec_d, int num_element, int k, int num_bucket, uint32_t* TopKElement, int NSubranges,
+    int SubRangesize, int alpha, double* timeforMaxsample, double* timeforFirstTopK, double* timeForsecondTopK,
+    double* timeforConcatenation, uint32_t* Max_d, int* SubrangeId_d, int beta, int defaultContribution,
+    int NthreadstoworkInreduction, int NThreadsPerBlock, int SizeOfAllocation, int NSharedMemoryElements,
+    int* SelectedSubrangeId_d, int* CountSelectedSubrange_d, int* CountLonelyElements_d, int* write_pos_d,
+    uint32_t* ConcatenatedRange_d) {
+  (void)Max_d; (void)SubrangeId_d; (void)NthreadstoworkInreduction; (void)NThreadsPerBlock; (void)SizeOfAllocation;
+  (void)NSharedMemoryElements; (void)SelectedSubrangeId_d; (void)ConcatenatedRange_d;
+  if (!vec_d || !TopKElement || num_element <= 0 || k <= 0 || k > num_element) return DRTOPK_EINVAL;
+  if (SubRangesize != (1 << alpha) || NSubranges != num_element / SubRangesize) return DRTOPK_EINVAL;
+  drtopk_params_t p;
+  drtopk_params_default(&p);
+  p.algo = DRTOPK_ALGO_BUCKET;
+  p.num_bucket = num_bucket;
+  p.alpha = alpha;
+  p.beta = beta;
+  p.path = defaultContribution ? 1 : 2;
+  drtopk_stats_t st;
+  drtopk_status_t s = blocking_select(vec_d, (uint64_t)num_element, (uint64_t)k, &p, TopKElement, &st);
+  if (s != DRTOPK_OK) return s;
+  if (timeforMaxsample) *timeforMaxsample = st.ms_sample * 1e-3;
+  if (timeforFirstTopK) *timeforFirstTopK = st.ms_first * 1e-3;
+  if (timeforConcatenation) *timeforConcatenation = st.ms_concat * 1e-3;
+  if (timeForsecondTopK) *timeForsecondTopK = st.ms_second * 1e-3;
+  int cnt[3] = {(int)st.n_selected, (int)st.n_lonely, (int)st.n_candidates};
+  if (CountSelectedSubrange_d) cudaMemcpy(CountSelectedSubrange_d, &cnt[0], 4, cudaMemcpyHostToDevice);
+  if (CountLonelyElements_d) cudaMemcpy(CountLonelyElements_d, &cnt[1], 4, cudaMemcpyHostToDevice);
+  if (write_pos_d) cudaMemcpy(write_pos_d, &cnt[2], 4, cudaMemcpyHostToDevice);
+  return DRTOPK_OK;
+}

@@ -1,0 +1,170 @@
+// common.cuh -- shared device helpers for the B200 Dr.Top-k kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define DRTOPK_DEV __device__ __forceinline__
+
+namespace drtopk {
+
+// ------------------------------------------------------------------ keys
+// Key modes: the kernels compare uint32 keys.  Float keys are mapped with the
+// order-preserving transform (negative -> bit-inverted, non-negative -> sign
+// bit set); "smallest" selection inverts the mapped key, so the same
+// largest-first machinery returns the k smallest.
+enum KeyMode : int { KM_U32 = 0, KM_F32 = 1, KM_U32_MIN = 2, KM_F32_MIN = 3 };
+
+template <int KM>
+DRTOPK_DEV uint32_t to_key(uint32_t u) {
+  if (KM == KM_F32 || KM == KM_F32_MIN) u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+  if (KM == KM_U32_MIN || KM == KM_F32_MIN) u = ~u;
+  return u;
+}
+
+DRTOPK_DEV uint32_t from_key(uint32_t k, int km) {
+  if (km == KM_U32_MIN || km == KM_F32_MIN) k = ~k;
+  if (km == KM_F32 || km == KM_F32_MIN) k = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+  return k;
+}
+
+// ------------------------------------------------------------------ loads
+// Streaming 128-bit load: read-only path, no L1 allocation, 256-byte L2
+// prefetch, and an L2 evict-first policy so the stream does not push the
+// (re-read) delegate vector out of L2.
+DRTOPK_DEV uint64_t make_evict_first_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
+DRTOPK_DEV uint4 ld_stream_v4(const uint32_t* p, uint64_t pol) {
+  uint4 r;
+  asm volatile(
+      "ld.global.nc.L1::no_allocate.L2::cache_hint.L2::256B.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+      : "l"(p), "l"(pol));
+  return r;
+}
+
+DRTOPK_DEV uint32_t ld_stream_u32(const uint32_t* p, uint64_t pol) {
+  uint32_t r;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(r) : "l"(p), "l"(pol));
+  return r;
+}
+
+// Loads of data written earlier in the same kernel (after a grid barrier):
+// must not use the non-coherent path.
+DRTOPK_DEV uint32_t ld_cg_u32(const uint32_t* p) {
+  uint32_t r;
+  asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(r) : "l"(p));
+  return r;
+}
+DRTOPK_DEV uint2 ld_cg_v2(const uint32_t* p) {
+  uint2 r;
+  asm volatile("ld.global.cg.v2.u32 {%0,%1}, [%2];" : "=r"(r.x), "=r"(r.y) : "l"(p));
+  return r;
+}
+DRTOPK_DEV uint4 ld_cg_v4(const uint32_t* p) {
+  uint4 r;
+  asm volatile("ld.global.cg.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w) : "l"(p));
+  return r;
+}
+
+DRTOPK_DEV uint64_t ld_cg_u64(const uint64_t* p) {
+  uint64_t r;
+  asm volatile("ld.global.cg.u64 %0, [%1];" : "=l"(r) : "l"(p));
+  return r;
+}
+
+DRTOPK_DEV uint32_t ld_acquire_gpu(const uint32_t* p) {
+  uint32_t r;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(r) : "l"(p) : "memory");
+  return r;
+}
+DRTOPK_DEV void st_release_gpu(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// ------------------------------------------------------------------ warp
+DRTOPK_DEV unsigned lane_id() { return threadIdx.x & 31u; }
+
+// Top-2 (multiset) merge of two (first, second) pairs.
+DRTOPK_DEV void top2_merge(uint32_t& a1, uint32_t& a2, uint32_t b1, uint32_t b2) {
+  uint32_t hi = max(a1, b1), lo = min(a1, b1);
+  a2 = max(lo, max(a2, b2));
+  a1 = hi;
+}
+DRTOPK_DEV void top2_push(uint32_t& a1, uint32_t& a2, uint32_t v) {
+  // same result as the reference's "if Max<v {Second=Max;Max=v} else if Second<v {Second=v}"
+  uint32_t lo = min(a1, v);
+  a1 = max(a1, v);
+  a2 = max(a2, lo);
+}
+
+// Warp-aggregated append: every lane with pred reserves one slot of *counter;
+// returns the slot (undefined for lanes without pred).  One atomic per warp.
+DRTOPK_DEV uint32_t warp_append(bool pred, uint32_t* counter) {
+  unsigned mask = __activemask();
+  unsigned b = __ballot_sync(mask, pred);
+  if (!b) return 0;
+  unsigned lane = lane_id();
+  int leader = __ffs(b) - 1;
+  uint32_t base = 0;
+  if ((int)lane == leader) base = atomicAdd(counter, (uint32_t)__popc(b));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(b & ((1u << lane) - 1u));
+}
+
+// ------------------------------------------------------------------ errors
+enum DevErr : uint32_t {
+  DE_BARRIER_TIMEOUT = 1u,   // a grid barrier gave up waiting
+  DE_OVERFLOW = 2u,          // a bounded buffer would have overflowed (skipped)
+  DE_INTERNAL = 4u,          // an invariant failed (result not trusted)
+};
+
+// Grid barrier for kernels launched cooperatively (all CTAs co-resident).
+// The spin is bounded: after ~2^26 polls (~seconds) the CTA records
+// DE_BARRIER_TIMEOUT and every later barrier returns false immediately, so a
+// broken launch ends with an error instead of a hang.
+struct GridBar {
+  uint32_t* count;   // arrivals in the current generation
+  uint32_t* gen;     // generation number
+  uint32_t* err;     // error word (host-visible)
+  uint32_t nblocks;
+};
+
+DRTOPK_DEV bool grid_barrier(const GridBar& gb) {
+  __shared__ uint32_t s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t ok = 1;
+    if (ld_acquire_gpu(gb.err) & DE_BARRIER_TIMEOUT) ok = 0;
+    if (ok) {
+      uint32_t g = ld_acquire_gpu(gb.gen);
+      __threadfence();
+      uint32_t arrived = atomicAdd(gb.count, 1u);
+      if (arrived == gb.nblocks - 1) {
+        atomicExch(gb.count, 0u);
+        __threadfence();
+        st_release_gpu(gb.gen, g + 1);
+      } else {
+        uint32_t it = 0;
+        while (ld_acquire_gpu(gb.gen) == g) {
+          if (++it > (1u << 26)) {
+            atomicOr(gb.err, (uint32_t)DE_BARRIER_TIMEOUT);
+            ok = 0;
+            break;
+          }
+          if ((it & 1023u) == 0 && (ld_acquire_gpu(gb.err) & DE_BARRIER_TIMEOUT)) { ok = 0; break; }
+          __nanosleep(64);
+        }
+      }
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+}  // namespace drtopk

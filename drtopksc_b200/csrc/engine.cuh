@@ -1,0 +1,369 @@
+// engine.cuh -- device-side k-th-largest select over (key, payload) sets,
+// shared by the first select (on delegates), the second select (on the
+// concatenated candidates), plain radix select and the integer bucket select.
+//
+// One "level" = pick a bin from the histogram of the current set, then split
+// the set: keys above the bin go to the top list, keys inside the bin form the
+// next set (compacted) and are histogrammed for the next level.
+//
+// Radix mode reproduces the reference's digit loop exactly
+// (baseline+filter+beta+shuffle/radixselect.cuh:191-220 CumulateCount_inplace,
+// 352-410 CalculateOccurence_inplace, 1410-1470 / 1666-1780 the host digit
+// loops): the bin chosen is the smallest i with CumCount[i] >= n-k+1, which is
+// the largest bin whose count-from-the-top reaches the remaining rank R.  The
+// range [lo,hi] of the chosen bin is the reference's flag with the digits
+// below still zero.  Bucket mode uses the same loop with integer bucket width
+// w = (hi-lo)/nb + 1 over a [min,max] range (exact restatement of
+// bucket_select/bucketselect_combined.cuh).
+//
+// All CTAs of the (cooperative) kernel execute the same sequence; the pick
+// is recomputed redundantly in every CTA from the global histogram, so the
+// replicated level state stays identical without extra broadcasts.
+#pragma once
+
+#include "common.cuh"
+
+namespace drtopk {
+
+constexpr int FUSED_THREADS = 256;
+constexpr int MAX_LEVELS = 40;
+
+struct EngineCfg {
+  int bucket;          // 0 radix, 1 bucket
+  int nbits;           // radix digit width
+  int nb;              // bins per level (1<<nbits, or bucket count <= 4096)
+  int stop_single;     // stop when the chosen bin holds exactly one key
+  int max_levels;      // stop after this many levels
+  int thr_only;        // only the final range is wanted (histogram passes, no appends)
+  int key_from_payload;  // key = ~payload (fill by lowest payload)
+};
+
+struct RunBufs {
+  uint32_t* H[3];       // rotating histograms (nb words each)
+  uint32_t* set_count;  // [MAX_LEVELS+2]: size of the set entering level j
+  uint2* cbuf[2];       // compact ping-pong buffers
+  uint2* top;           // top list (capacity k)
+  uint32_t* top_count;
+};
+
+struct Level {
+  uint32_t lo, hi;  // range of the set entering this level (inclusive)
+  uint32_t w;       // bucket width at this level
+  int wshift;       // log2(w) in radix mode, -1 in bucket mode
+  uint32_t R;       // remaining rank within the range
+};
+
+// Source set of a run: either a key array with implicit payload (index) or
+// an array of (key, payload) pairs.
+struct Src {
+  const uint32_t* keys;   // form 1
+  const uint2* pairs;     // form 2
+  uint64_t count;         // form 1 count (host-known)
+  const uint32_t* count_dev;  // form 2 count (device)
+  int raw_input;          // form 1 keys are the raw input (apply key transform)
+};
+
+struct RunResult {
+  uint32_t thr;     // final range lower bound
+  uint32_t kth;     // exact k-th key when the run finished (collapse/single)
+  int levels;
+  int ok;
+};
+
+DRTOPK_DEV uint32_t bin_of(uint32_t k, uint32_t lo, uint32_t w, int wshift) {
+  uint32_t d = k - lo;
+  return wshift >= 0 ? (d >> wshift) : (d / w);
+}
+
+// --------------------------------------------------------------- block pick
+struct Pick {
+  uint32_t b, cnt, above;
+};
+
+// Every CTA: find the largest bin b with (count of bins >= b) >= R.
+DRTOPK_DEV Pick block_pick(const uint32_t* H, int nb, uint32_t R) {
+  __shared__ uint32_t s_part[FUSED_THREADS / 32];
+  __shared__ Pick s_pick;
+  __shared__ int s_found;
+  const int t = threadIdx.x;
+  const int q = (nb + FUSED_THREADS - 1) / FUSED_THREADS;
+  const int b0 = min(nb, t * q), b1 = min(nb, b0 + q);
+  uint32_t local = 0;
+  for (int b = b0; b < b1; ++b) local += ld_cg_u32(H + b);
+  // inclusive prefix over threads (ascending), then above_t = total - incl
+  uint32_t incl = local;
+  const unsigned lane = t & 31u;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+    if ((int)lane >= off) incl += y;
+  }
+  if (lane == 31) s_part[t >> 5] = incl;
+  if (t == 0) s_found = 0;
+  __syncthreads();
+  uint32_t wbase = 0, total = 0;
+  for (int w = 0; w < FUSED_THREADS / 32; ++w) {
+    if (w < (t >> 5)) wbase += s_part[w];
+    total += s_part[w];
+  }
+  incl += wbase;
+  const uint32_t above_t = total - incl;
+  if (local > 0 && above_t < R && R <= above_t + local) {
+    uint32_t acc = above_t;
+    for (int b = b1 - 1; b >= b0; --b) {
+      uint32_t c = ld_cg_u32(H + b);
+      if (acc + c >= R) {
+        s_pick.b = b; s_pick.cnt = c; s_pick.above = acc;
+        s_found = 1;
+        break;
+      }
+      acc += c;
+    }
+  }
+  __syncthreads();
+  Pick p;
+  if (s_found) p = s_pick;
+  else {  // R exceeds the set: the reference's rule then picks bin 0
+    uint32_t h0 = ld_cg_u32(H);
+    p.b = 0; p.cnt = h0; p.above = total - h0;
+  }
+  __syncthreads();
+  return p;
+}
+
+// next level state after picking bin p from level L; returns done flag
+DRTOPK_DEV bool advance(const EngineCfg& c, const Level& L, const Pick& p, int level_index, Level& N) {
+  uint64_t lo2 = (uint64_t)L.lo + (uint64_t)p.b * (uint64_t)L.w;
+  uint64_t hi2 = min((uint64_t)L.hi, lo2 + (uint64_t)L.w - 1);
+  N.lo = (uint32_t)lo2;
+  N.hi = (uint32_t)hi2;
+  N.R = L.R - p.above;
+  if (c.bucket) {
+    N.wshift = -1;
+    N.w = (uint32_t)((uint64_t)(N.hi - N.lo) / (uint64_t)c.nb + 1);
+  } else {
+    N.wshift = L.wshift - c.nbits;
+    N.w = N.wshift >= 0 ? (1u << N.wshift) : 1u;
+  }
+  bool done = (N.lo == N.hi) || (c.stop_single && p.cnt == 1) || (level_index + 1 >= c.max_levels);
+  return done;
+}
+
+// --------------------------------------------------------------- helpers
+DRTOPK_DEV void zero_words(uint32_t* p, int n) {
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = g; i < (uint64_t)n; i += G) p[i] = 0;
+}
+
+DRTOPK_DEV void flush_hist(uint32_t* s_hist, uint32_t* gH, int nb) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    uint32_t v = s_hist[i];
+    if (v) atomicAdd(gH + i, v);
+  }
+  __syncthreads();
+}
+
+DRTOPK_DEV void clear_hist(uint32_t* s_hist, int nb) {
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) s_hist[i] = 0;
+  __syncthreads();
+}
+
+template <int KM>
+DRTOPK_DEV uint32_t src_key1(const Src& s, uint64_t i) {
+  uint32_t v = ld_cg_u32(s.keys + i);
+  return s.raw_input ? to_key<KM>(v) : v;
+}
+
+// entry visitor over the source set (grid-stride, warp-uniform trip count).
+// fn(key, payload, valid) is called for every slot; valid=false for padding.
+template <int KM, typename F>
+DRTOPK_DEV void for_each_src(const Src& s, bool from_pairs, uint64_t count, F&& fn) {
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t iters = (count + G - 1) / G;
+  for (uint64_t it = 0; it < iters; ++it) {
+    const uint64_t i = it * G + g;
+    const bool valid = i < count;
+    uint32_t key = 0, pay = 0;
+    if (valid) {
+      if (from_pairs) {
+        uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(s.pairs + i));
+        key = e.x; pay = e.y;
+      } else {
+        key = src_key1<KM>(s, i);
+        pay = (uint32_t)i;
+      }
+    }
+    fn(key, pay, valid);
+  }
+}
+
+// --------------------------------------------------------------- one run
+// Runs levels until done.  H[0] of the run must hold the histogram of level
+// 0 over the source (with range L0) and H[1] must be zero when called.
+// Barrier after every level.  Appends the keys above the final range to
+// rb.top; leaves the final range's members in a compact buffer.
+// Returns the level index that finished and the final Level through Lout.
+template <int KM>
+DRTOPK_DEV int run_levels(const EngineCfg& c, const Src& src0, bool src0_pairs, const RunBufs& rb, Level L,
+                          uint32_t* s_hist, const GridBar& gb, Level& Lout, Pick& last_pick, int& eq_buf,
+                          uint64_t& eq_count, bool& ok) {
+  int j = 0;
+  ok = true;
+  for (;; ++j) {
+    if (j >= MAX_LEVELS) { ok = false; break; }
+    Pick p = block_pick(rb.H[j % 3], c.nb, L.R);
+    Level N;
+    bool done = advance(c, L, p, j, N);
+    last_pick = p;
+    zero_words(rb.H[(j + 2) % 3], c.nb);
+    uint32_t* Hn = rb.H[(j + 1) % 3];
+    const bool want_hist = !done;
+    clear_hist(s_hist, c.nb);
+    if (c.thr_only) {
+      if (done) { Lout = N; break; }
+      // histogram the members of the new range over the level-0 source
+      const uint64_t cnt = src0_pairs ? (uint64_t)ld_cg_u32(src0.count_dev) : src0.count;
+      for_each_src<KM>(src0, src0_pairs, cnt, [&](uint32_t key, uint32_t, bool valid) {
+        if (valid && key >= N.lo && key <= N.hi) atomicAdd(&s_hist[bin_of(key, N.lo, N.w, N.wshift)], 1u);
+      });
+      flush_hist(s_hist, Hn, c.nb);
+      if (!grid_barrier(gb)) { ok = false; break; }
+      L = N;
+      continue;
+    }
+    // split
+    const bool from_pairs = (j == 0) ? src0_pairs : true;
+    Src s = src0;
+    uint64_t cnt;
+    bool filter;
+    if (j == 0) {
+      cnt = src0_pairs ? (uint64_t)ld_cg_u32(src0.count_dev) : src0.count;
+      filter = false;  // level 0 range covers the whole source
+    } else {
+      s.pairs = rb.cbuf[(j - 1) & 1];
+      cnt = ld_cg_u32(rb.set_count + j);
+      filter = false;
+    }
+    uint2* nxt = rb.cbuf[j & 1];
+    uint32_t* nxt_cnt = rb.set_count + j + 1;
+    const bool kfp = c.key_from_payload;
+    for_each_src<KM>(s, from_pairs, cnt, [&](uint32_t val, uint32_t pay, bool valid) {
+      const uint32_t key = kfp ? ~pay : val;
+      const bool member = valid && (!filter || (key >= L.lo && key <= L.hi));
+      const bool up = member && key > N.hi;
+      const bool in = member && key >= N.lo && key <= N.hi;
+      uint32_t slot = warp_append(up, rb.top_count);
+      if (up) rb.top[slot] = make_uint2(val, pay);
+      uint32_t slot2 = warp_append(in, nxt_cnt);
+      if (in) {
+        nxt[slot2] = make_uint2(val, pay);
+        if (want_hist) atomicAdd(&s_hist[bin_of(key, N.lo, N.w, N.wshift)], 1u);
+      }
+    });
+    if (want_hist) flush_hist(s_hist, Hn, c.nb);
+    if (!grid_barrier(gb)) { ok = false; break; }
+    L = N;
+    if (done) {
+      Lout = N;
+      eq_buf = j & 1;
+      eq_count = ld_cg_u32(rb.set_count + j + 1);
+      break;
+    }
+  }
+  return j;
+}
+
+// histogram pass of level 0 for a run: hist of bin_of(key, L0) over the source
+template <int KM>
+DRTOPK_DEV void hist_pass(const Src& src, bool pairs, bool key_from_payload, const Level& L0, int nb, uint32_t* gH,
+                          uint32_t* s_hist) {
+  clear_hist(s_hist, nb);
+  const uint64_t cnt = pairs ? (uint64_t)ld_cg_u32(src.count_dev) : src.count;
+  for_each_src<KM>(src, pairs, cnt, [&](uint32_t val, uint32_t pay, bool valid) {
+    const uint32_t key = key_from_payload ? ~pay : val;
+    if (valid && key >= L0.lo && key <= L0.hi) atomicAdd(&s_hist[bin_of(key, L0.lo, L0.w, L0.wshift)], 1u);
+  });
+  flush_hist(s_hist, gH, nb);
+}
+
+DRTOPK_DEV Level radix_level0(int nbits, uint32_t R) {
+  Level L;
+  L.lo = 0; L.hi = 0xffffffffu; L.wshift = 32 - nbits; L.w = 1u << L.wshift; L.R = R;
+  return L;
+}
+
+DRTOPK_DEV Level bucket_level0(uint32_t mn, uint32_t mx, int nb, uint32_t R) {
+  Level L;
+  L.lo = mn; L.hi = mx; L.wshift = -1;
+  L.w = (uint32_t)((uint64_t)(mx - mn) / (uint64_t)nb + 1);
+  L.R = R;
+  return L;
+}
+
+// Full select run: levels, then the tie fill (lowest payloads among the
+// keys equal to the k-th) so that rb.top ends with exactly R0 entries.
+// fb: buffers of the fill sub-run (its own histograms and counts; its
+// compact buffers alias rb's).
+template <int KM>
+DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_pairs, const RunBufs& rb,
+                                const RunBufs& fb, Level L0, uint32_t* s_hist, const GridBar& gb) {
+  RunResult res = {0u, 0u, 0, 1};
+  Level Lf;
+  Pick lp;
+  int eqb = 0;
+  uint64_t E = 0;
+  bool ok = true;
+  int j = run_levels<KM>(c, src0, src0_pairs, rb, L0, s_hist, gb, Lf, lp, eqb, E, ok);
+  res.levels = j + 1;
+  res.thr = Lf.lo;
+  if (!ok) { res.ok = 0; return res; }
+  if (c.thr_only) return res;
+  const uint2* eq = rb.cbuf[eqb];
+  res.kth = (E == 1) ? ld_cg_v2(reinterpret_cast<const uint32_t*>(eq)).x : Lf.lo;
+  const uint32_t R = Lf.R;
+  if (E == R) {
+    Src s = {};
+    s.pairs = eq;
+    for_each_src<KM>(s, true, E, [&](uint32_t val, uint32_t pay, bool valid) {
+      uint32_t slot = warp_append(valid, rb.top_count);
+      if (valid) rb.top[slot] = make_uint2(val, pay);
+    });
+    if (!grid_barrier(gb)) res.ok = 0;
+    return res;
+  }
+  if (E < R) { res.ok = 0; return res; }
+  // E > R: keep the R lowest payloads among the tied entries (key = ~payload)
+  EngineCfg fc = {0, 8, 256, 1, 4, 0, 1};
+  Src s = {};
+  s.pairs = eq;
+  s.count_dev = rb.set_count + j + 1;
+  Level F0 = radix_level0(8, R);
+  hist_pass<KM>(s, true, true, F0, 256, fb.H[0], s_hist);
+  if (!grid_barrier(gb)) { res.ok = 0; return res; }
+  RunBufs fr = fb;
+  fr.cbuf[0] = rb.cbuf[eqb ^ 1];
+  fr.cbuf[1] = rb.cbuf[eqb];
+  fr.top = rb.top;
+  fr.top_count = rb.top_count;
+  Level Lf2;
+  Pick lp2;
+  int eqb2 = 0;
+  uint64_t E2 = 0;
+  bool ok2 = true;
+  int j2 = run_levels<KM>(fc, s, true, fr, F0, s_hist, gb, Lf2, lp2, eqb2, E2, ok2);
+  (void)j2;
+  if (!ok2 || E2 != 1 || Lf2.R != 1) { res.ok = 0; return res; }
+  // append the single remaining entry
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(fr.cbuf[eqb2]));
+    uint32_t slot = atomicAdd(rb.top_count, 1u);
+    rb.top[slot] = e;
+  }
+  if (!grid_barrier(gb)) res.ok = 0;
+  return res;
+}
+
+}  // namespace drtopk

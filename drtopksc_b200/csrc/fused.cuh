@@ -1,0 +1,507 @@
+// fused.cuh -- everything after the delegate sampler, in one persistent
+// cooperative kernel with grid barriers between phases (no host round trip;
+// the reference makes ~30 synchronous calls here: radixselect.cuh:1782-1894).
+//
+//   phase 1  first select on the delegates
+//            default path (beta=1): k-th largest delegate with the reference's
+//            early stop; the k subranges kept are those above the final range
+//            plus the lowest-id ties (FindTopKRanges 412-427 +
+//            FillWithKElementsID 602-618, made deterministic).
+//            beta path (beta=2): threshold only, from the top digits of the
+//            (Max, Second) delegates (radix_select_inplace_firsttopk_beta
+//            1727-1780).
+//   phase 2  concatenation of candidates >= threshold
+//            default: keys of the k kept subranges (CreateConcatenateRange_
+//            optimized 1574-1607); beta: FindTopKRanges_beta 560-598 (Max and
+//            Second >= thr -> whole subrange; Max only -> that one key) fused
+//            with CreateConcatenateRange_Beta_optimized 1609-1639.  Appends
+//            are warp-aggregated; the same pass histograms the candidates'
+//            top digit (first level of phase 3).
+//   phase 3  second select over the candidates (radix_select_inplace
+//            1410-1470): exact k-th largest, plus the top-k list with ties
+//            broken by lowest index.
+//   phase 4  output: k-th value, top-k values/indices (optionally sorted by
+//            value desc, index asc).
+#pragma once
+
+#include "engine.cuh"
+
+namespace drtopk {
+
+enum Path : int { PATH_DEFAULT = 0, PATH_BETA = 1, PATH_PLAIN = 2 };
+
+constexpr int SMALL_SORT = 4096;  // top-k sorted in one CTA's shared memory up to this k
+
+struct FusedArgs {
+  const uint32_t* keys;
+  uint64_t n;
+  uint32_t k;
+  int km;
+  int path;
+  int bucket;
+  int nbits;
+  int nb;
+  int alpha;
+  uint64_t M;
+  int first_levels;  // level cap of the first select (beta path threshold levels)
+  int vec_ok;
+  const uint32_t* del;
+  const uint16_t* pos;
+  int has_pos;
+  const uint32_t* del_minmax;  // [2] from the sampler (bucket mode)
+  RunBufs A, AF, C, CF;
+  uint2* cand;
+  uint32_t* cand_count;
+  uint64_t cand_cap;
+  uint32_t* cand_minmax;  // [2] (bucket mode)
+  uint32_t* out_kth;      // [1] original value bits
+  uint32_t* out_vals;     // [k] or null
+  int64_t* out_idx;       // [k] or null
+  int sorted;
+  uint64_t* sort_buf[2];  // [k] each (large sorted output)
+  uint32_t* sort_cnt;     // [grid][256]
+  uint32_t* sort_tot;     // [8][256]
+  uint32_t* stats;        // [16]
+  GridBar gb;
+};
+
+enum StatSlot : int {
+  ST_THR1 = 0, ST_NSEL = 1, ST_NLONELY = 2, ST_NCAND = 3, ST_LVA = 4, ST_LVC = 5,
+  ST_TOPA = 6, ST_TOPC = 7, ST_KTH = 8, ST_OK = 9
+};
+
+// --------------------------------------------------------------- gathers
+template <int KM>
+DRTOPK_DEV void emit_candidate(const FusedArgs& a, bool take, uint32_t key, uint32_t idx, uint32_t* s_hist,
+                               uint32_t& mlo, uint32_t& mhi, bool& ovf) {
+  uint32_t slot = warp_append(take, a.cand_count);
+  if (take) {
+    if (slot < a.cand_cap) a.cand[slot] = make_uint2(key, idx);
+    else ovf = true;
+    if (a.bucket) { mlo = max(mlo, ~key); mhi = max(mhi, key); }
+    else atomicAdd(&s_hist[key >> (32 - a.nbits)], 1u);
+  }
+}
+
+template <int KM>
+DRTOPK_DEV void load4(const FusedArgs& a, uint64_t base, bool vec, uint32_t (&v)[4]) {
+  if (vec) {
+    uint4 q = __ldg(reinterpret_cast<const uint4*>(a.keys + base));
+    v[0] = to_key<KM>(q.x); v[1] = to_key<KM>(q.y); v[2] = to_key<KM>(q.z); v[3] = to_key<KM>(q.w);
+  } else {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) v[e] = (base + e < a.n) ? to_key<KM>(__ldg(a.keys + base + e)) : 0u;
+  }
+}
+
+// default path: keys >= thr of the k kept subranges (uint4 granules, S >= 4)
+template <int KM>
+DRTOPK_DEV void gather_default(const FusedArgs& a, uint32_t thr, uint32_t* s_hist, uint32_t& mlo, uint32_t& mhi,
+                               bool& ovf) {
+  const uint64_t S = 1ull << a.alpha;
+  const uint64_t units = ((uint64_t)a.k * S) >> 2;
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t iters = (units + G - 1) / G;
+  for (uint64_t it = 0; it < iters; ++it) {
+    const uint64_t u = it * G + g;
+    bool valid = u < units;
+    uint64_t base = 0;
+    uint32_t v[4] = {0u, 0u, 0u, 0u};
+    if (valid) {
+      const uint64_t q = u << 2;
+      const uint64_t sel = q >> a.alpha;
+      const uint32_t sub = ld_cg_v2(reinterpret_cast<const uint32_t*>(a.A.top + sel)).y;
+      base = ((uint64_t)sub << a.alpha) + (q & (S - 1));
+      load4<KM>(a, base, a.vec_ok && base + 4 <= a.n, v);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const bool take = valid && (base + e < a.n) && v[e] >= thr;
+      emit_candidate<KM>(a, take, v[e], (uint32_t)(base + e), s_hist, mlo, mhi, ovf);
+    }
+  }
+}
+
+// beta path: FindTopKRanges_beta fused with the concatenation
+template <int KM>
+DRTOPK_DEV void filter_gather_beta(const FusedArgs& a, uint32_t thr, uint32_t* s_hist, uint32_t& mlo, uint32_t& mhi,
+                                   bool& ovf, uint32_t& nsel, uint32_t& nlonely) {
+  const uint64_t S = 1ull << a.alpha;
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t iters = (a.M + G - 1) / G;
+  for (uint64_t it = 0; it < iters; ++it) {
+    const uint64_t j = it * G + g;
+    bool sel = false, lonely = false;
+    uint32_t m1 = 0;
+    if (j < a.M) {
+      uint2 d = *reinterpret_cast<const uint2*>(a.del + 2 * j);
+      m1 = d.x;
+      sel = d.x >= thr && d.y >= thr;
+      lonely = d.x >= thr && d.y < thr;
+    }
+    nsel += sel;
+    nlonely += lonely;
+    const uint64_t jb = j << a.alpha;
+    uint32_t lidx = (uint32_t)jb;
+    if (lonely && a.has_pos) lidx += a.pos[j];
+    emit_candidate<KM>(a, lonely, m1, lidx, s_hist, mlo, mhi, ovf);
+    if (__any_sync(0xffffffffu, sel)) {
+      for (uint64_t e = 0; e < S; e += 4) {
+        uint32_t v[4] = {0u, 0u, 0u, 0u};
+        if (sel) {
+          if (S >= 4) load4<KM>(a, jb + e, a.vec_ok && jb + e + 4 <= a.n, v);
+          else
+            for (int t = 0; t < (int)S; ++t) v[t] = (jb + t < a.n) ? to_key<KM>(__ldg(a.keys + jb + t)) : 0u;
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const bool take = sel && (e + t < S) && (jb + e + t < a.n) && v[t] >= thr;
+          emit_candidate<KM>(a, take, v[t], (uint32_t)(jb + e + t), s_hist, mlo, mhi, ovf);
+        }
+      }
+    }
+  }
+}
+
+// min/max pass over a key array (plain bucket path)
+template <int KM>
+DRTOPK_DEV void minmax_pass(const FusedArgs& a, uint32_t* gmm) {
+  __shared__ uint32_t s_mm[2];
+  if (threadIdx.x < 2) s_mm[threadIdx.x] = 0;
+  __syncthreads();
+  uint32_t lo = 0, hi = 0;
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = g; i < a.n; i += G) {
+    uint32_t k = to_key<KM>(__ldg(a.keys + i));
+    lo = max(lo, ~k);
+    hi = max(hi, k);
+  }
+  atomicMax(&s_mm[0], lo);
+  atomicMax(&s_mm[1], hi);
+  __syncthreads();
+  if (threadIdx.x == 0) { atomicMax(&gmm[0], s_mm[0]); atomicMax(&gmm[1], s_mm[1]); }
+}
+
+// --------------------------------------------------------------- sorting
+// One CTA: bitonic sort of n64 (<= SMALL_SORT, padded to a power of two)
+// 64-bit composites in shared memory, descending.
+DRTOPK_DEV void block_bitonic_desc(uint64_t* s, int npow2) {
+  for (int size = 2; size <= npow2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < npow2 / 2; i += blockDim.x) {
+        int lo = 2 * stride * (i / stride) + (i % stride);
+        int hi = lo + stride;
+        bool desc = ((lo & size) == 0);
+        uint64_t x = s[lo], y = s[hi];
+        if ((x < y) == desc) { s[lo] = y; s[hi] = x; }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Multi-CTA stable LSD radix sort of nk 64-bit keys ascending (8-bit
+// digits), skipping digits that are constant over all keys.  Keys are
+// (~value << 32) | index, so ascending order = value desc, index asc.
+// Each CTA owns one contiguous range; per digit: CTA counts -> column scan
+// over CTAs (one digit column per CTA) -> stable scatter.  Returns the
+// buffer holding the result.
+DRTOPK_DEV uint64_t* grid_lsd_sort(const FusedArgs& a, uint64_t* src, uint64_t* dst, uint32_t nk, uint32_t* s_cnt,
+                                   bool& ok) {
+  const int C = gridDim.x, c = blockIdx.x, t = threadIdx.x;
+  const uint32_t per = (nk + C - 1) / C;
+  const uint32_t r0 = min(nk, per * c), r1 = min(nk, r0 + per);
+  // totals of all 8 digits
+  for (int d = 0; d < 8; ++d) {
+    for (int i = t; i < 256; i += blockDim.x) s_cnt[i] = 0;
+    __syncthreads();
+    for (uint32_t i = r0 + t; i < r1; i += blockDim.x) atomicAdd(&s_cnt[(ld_cg_u64(src + i) >> (8 * d)) & 255u], 1u);
+    __syncthreads();
+    for (int i = t; i < 256; i += blockDim.x)
+      if (s_cnt[i]) atomicAdd(&a.sort_tot[d * 256 + i], s_cnt[i]);
+    __syncthreads();
+  }
+  if (!grid_barrier(a.gb)) { ok = false; return src; }
+  __shared__ uint32_t s_run[256];
+  __shared__ uint32_t s_wcnt[FUSED_THREADS / 32][257];
+  __shared__ int s_trivial;
+  for (int d = 0; d < 8; ++d) {
+    if (t == 0) s_trivial = 0;
+    __syncthreads();
+    for (int i = t; i < 256; i += blockDim.x)
+      if (ld_cg_u32(a.sort_tot + d * 256 + i) == nk) s_trivial = 1;
+    __syncthreads();
+    if (s_trivial) continue;
+    const int sh = 8 * d;
+    // 1) this CTA's digit counts
+    for (int i = t; i < 256; i += blockDim.x) s_cnt[i] = 0;
+    __syncthreads();
+    for (uint32_t i = r0 + t; i < r1; i += blockDim.x) atomicAdd(&s_cnt[(ld_cg_u64(src + i) >> sh) & 255u], 1u);
+    __syncthreads();
+    for (int i = t; i < 256; i += blockDim.x) a.sort_cnt[(uint64_t)c * 256 + i] = s_cnt[i];
+    if (!grid_barrier(a.gb)) { ok = false; return src; }
+    // 2) exclusive scan of each digit column over the CTAs (in place)
+    for (int col = c; col < 256; col += C) {
+      if (t < 32) {
+        uint32_t carry = 0;
+        for (int c0 = 0; c0 < C; c0 += 32) {
+          const int cc = c0 + t;
+          uint32_t v = cc < C ? ld_cg_u32(a.sort_cnt + (uint64_t)cc * 256 + col) : 0u;
+          uint32_t incl = v;
+#pragma unroll
+          for (int off = 1; off < 32; off <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+            if (t >= off) incl += y;
+          }
+          if (cc < C) a.sort_cnt[(uint64_t)cc * 256 + col] = carry + incl - v;
+          carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+      }
+    }
+    if (!grid_barrier(a.gb)) { ok = false; return src; }
+    // 3) running offsets = digit base (scan of totals) + this CTA's column prefix
+    if (t < 256) s_cnt[t] = ld_cg_u32(a.sort_tot + d * 256 + t);
+    __syncthreads();
+    if (t == 0) {
+      uint32_t acc = 0;
+      for (int i = 0; i < 256; ++i) { uint32_t v = s_cnt[i]; s_cnt[i] = acc; acc += v; }
+    }
+    __syncthreads();
+    if (t < 256) s_run[t] = s_cnt[t] + ld_cg_u32(a.sort_cnt + (uint64_t)c * 256 + t);
+    __syncthreads();
+    // 4) stable scatter in chunks of blockDim keys
+    const int wid = t >> 5;
+    const unsigned lane = t & 31u;
+    for (uint32_t cb = r0; cb < r1; cb += blockDim.x) {
+      const uint32_t i = cb + t;
+      const bool valid = i < r1;
+      const uint64_t key = valid ? ld_cg_u64(src + i) : 0ull;
+      const uint32_t dg = valid ? (uint32_t)((key >> sh) & 255u) : 256u;
+      for (int q = lane; q < 257; q += 32) s_wcnt[wid][q] = 0;
+      __syncwarp();
+      const unsigned peers = __match_any_sync(0xffffffffu, dg);
+      const uint32_t rank_in_warp = __popc(peers & ((1u << lane) - 1u));
+      if (rank_in_warp == 0) s_wcnt[wid][dg] = __popc(peers);
+      __syncthreads();
+      if (valid) {
+        uint32_t before_w = 0;
+        for (int w2 = 0; w2 < wid; ++w2) before_w += s_wcnt[w2][dg];
+        dst[s_run[dg] + before_w + rank_in_warp] = key;
+      }
+      __syncthreads();
+      for (int q = t; q < 256; q += blockDim.x) {
+        uint32_t add = 0;
+        for (int w2 = 0; w2 < FUSED_THREADS / 32; ++w2) add += s_wcnt[w2][q];
+        s_run[q] += add;
+      }
+      __syncthreads();
+    }
+    if (!grid_barrier(a.gb)) { ok = false; return src; }
+    uint64_t* tmp = src; src = dst; dst = tmp;
+  }
+  return src;
+}
+
+DRTOPK_DEV void stamp(uint32_t* stats, int slot) {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  stats[slot] = (uint32_t)t;
+  stats[slot + 1] = (uint32_t)(t >> 32);
+}
+
+// --------------------------------------------------------------- kernel
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  uint32_t* s_hist = s_dyn;
+  const GridBar& gb = a.gb;
+  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  const int D = 32 / a.nbits;
+  uint32_t thr1 = 0, nsel = 0, nlonely = 0;
+  int lvA = 0;
+  if (lead) stamp(a.stats, 16);
+
+  // ---------------- phase 1: first select on the delegates
+  if (a.path == PATH_DEFAULT || a.path == PATH_BETA) {
+    const uint64_t ndel = a.path == PATH_BETA ? 2 * a.M : a.M;
+    Src s = {};
+    s.keys = a.del;
+    s.count = ndel;
+    Level L0;
+    if (a.bucket) {
+      L0 = bucket_level0(~ld_cg_u32(a.del_minmax), ld_cg_u32(a.del_minmax + 1), a.nb, a.k);
+      hist_pass<KM>(s, false, false, L0, a.nb, a.A.H[0], s_hist);
+      if (!grid_barrier(gb)) return;
+    } else {
+      L0 = radix_level0(a.nbits, a.k);
+    }
+    EngineCfg c;
+    c.bucket = a.bucket; c.nbits = a.nbits; c.nb = a.nb; c.key_from_payload = 0;
+    if (a.path == PATH_DEFAULT) {
+      c.stop_single = 1; c.thr_only = 0;
+      c.max_levels = a.bucket ? MAX_LEVELS : D;
+    } else {
+      c.stop_single = 0; c.thr_only = 1;
+      c.max_levels = a.first_levels;
+    }
+    if (a.path == PATH_BETA && c.max_levels <= 0) {
+      thr1 = 0;  // no digit processed: every subrange qualifies
+    } else {
+      RunResult r = run_select<KM>(c, s, false, a.A, a.AF, L0, s_hist, gb);
+      if (!r.ok) { if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL); return; }
+      lvA = r.levels;
+      // radix keeps the reference's flag (final range lower bound); the bucket
+      // variant uses the exact k-th delegate on its default path
+      thr1 = (a.path == PATH_DEFAULT && a.bucket) ? r.kth : r.thr;
+    }
+  }
+
+  // ---------------- phase 2: concatenation of candidates
+  if (lead) stamp(a.stats, 18);
+  clear_hist(s_hist, a.nb);
+  uint32_t mlo = 0, mhi = 0;
+  bool ovf = false;
+  if (a.path == PATH_DEFAULT) {
+    // the k kept subranges must all be there before their ids are used as
+    // addresses (every CTA reads the same count after the last barrier)
+    if (ld_cg_u32(a.A.top_count) != a.k) {
+      if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
+      return;
+    }
+    gather_default<KM>(a, thr1, s_hist, mlo, mhi, ovf);
+    nsel = a.k;
+  } else if (a.path == PATH_BETA) {
+    filter_gather_beta<KM>(a, thr1, s_hist, mlo, mhi, ovf, nsel, nlonely);
+  }
+  if (ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
+  if (a.path != PATH_PLAIN) {
+    if (a.bucket) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        mlo = max(mlo, __shfl_xor_sync(0xffffffffu, mlo, off));
+        mhi = max(mhi, __shfl_xor_sync(0xffffffffu, mhi, off));
+      }
+      if ((threadIdx.x & 31) == 0) { atomicMax(&a.cand_minmax[0], mlo); atomicMax(&a.cand_minmax[1], mhi); }
+    } else {
+      flush_hist(s_hist, a.C.H[0], a.nb);
+    }
+    // selection statistics (n_selected summed over threads)
+    for (int off = 16; off > 0; off >>= 1) {
+      nsel += __shfl_xor_sync(0xffffffffu, nsel, off);
+      nlonely += __shfl_xor_sync(0xffffffffu, nlonely, off);
+    }
+    if ((threadIdx.x & 31) == 0 && a.path == PATH_BETA) {
+      atomicAdd(&a.stats[ST_NSEL], nsel);
+      atomicAdd(&a.stats[ST_NLONELY], nlonely);
+    }
+  } else {
+    // plain select: level-0 statistics straight off the input
+    if (a.bucket) minmax_pass<KM>(a, a.cand_minmax);
+    else {
+      Src s = {};
+      s.keys = a.keys; s.count = a.n; s.raw_input = 1;
+      hist_pass<KM>(s, false, false, radix_level0(a.nbits, a.k), a.nb, a.C.H[0], s_hist);
+    }
+  }
+  if (!grid_barrier(gb)) return;
+
+  // ---------------- phase 3: second select
+  if (lead) stamp(a.stats, 20);
+  Src sc = {};
+  bool pairs;
+  if (a.path == PATH_PLAIN) {
+    sc.keys = a.keys; sc.count = a.n; sc.raw_input = 1;
+    pairs = false;
+  } else {
+    sc.pairs = a.cand; sc.count_dev = a.cand_count;
+    pairs = true;
+    if (ld_cg_u32(a.cand_count) < a.k || ld_cg_u32(a.cand_count) > a.cand_cap) {
+      if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
+      return;
+    }
+  }
+  Level L0c;
+  if (a.bucket) {
+    L0c = bucket_level0(~ld_cg_u32(a.cand_minmax), ld_cg_u32(a.cand_minmax + 1), a.nb, a.k);
+    hist_pass<KM>(sc, pairs, false, L0c, a.nb, a.C.H[0], s_hist);
+    if (!grid_barrier(gb)) return;
+  } else {
+    L0c = radix_level0(a.nbits, a.k);
+  }
+  EngineCfg cc;
+  cc.bucket = a.bucket; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
+  cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0;
+  RunResult rc = run_select<KM>(cc, sc, pairs, a.C, a.CF, L0c, s_hist, gb);
+  if (!rc.ok) { if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL); return; }
+  const uint32_t K = rc.kth;
+  const uint32_t ntop = ld_cg_u32(a.C.top_count);
+  if (lead) {
+    stamp(a.stats, 22);
+    if (a.out_kth) a.out_kth[0] = from_key(K, a.km);
+    a.stats[ST_THR1] = thr1;
+    if (a.path == PATH_DEFAULT) a.stats[ST_NSEL] = a.k;
+    a.stats[ST_NCAND] = a.path == PATH_PLAIN ? (uint32_t)a.n : ld_cg_u32(a.cand_count);
+    a.stats[ST_LVA] = lvA;
+    a.stats[ST_LVC] = rc.levels;
+    a.stats[ST_TOPA] = a.path == PATH_DEFAULT ? ld_cg_u32(a.A.top_count) : 0u;
+    a.stats[ST_TOPC] = ntop;
+    a.stats[ST_KTH] = K;
+    a.stats[ST_OK] = 1;
+    if (ntop != a.k) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
+  }
+  if (!a.out_vals && !a.out_idx) return;
+  if (ntop != a.k) return;
+
+  // ---------------- phase 4: top-k output
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+  if (!a.sorted) {
+    for (uint64_t i = g; i < a.k; i += G) {
+      uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i));
+      if (a.out_vals) a.out_vals[i] = from_key(e.x, a.km);
+      if (a.out_idx) a.out_idx[i] = (int64_t)e.y;
+    }
+    return;
+  }
+  if (a.k <= SMALL_SORT) {
+    if (blockIdx.x != 0) return;
+    uint64_t* s = reinterpret_cast<uint64_t*>(s_dyn);
+    int np2 = 1;
+    while (np2 < (int)a.k) np2 <<= 1;
+    for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+      uint64_t v = 0;
+      if (i < (int)a.k) {
+        uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i));
+        v = ((uint64_t)e.x << 32) | (uint64_t)(~e.y);
+      }
+      s[i] = v;
+    }
+    block_bitonic_desc(s, np2);
+    for (int i = threadIdx.x; i < (int)a.k; i += blockDim.x) {
+      uint64_t v = s[i];
+      if (a.out_vals) a.out_vals[i] = from_key((uint32_t)(v >> 32), a.km);
+      if (a.out_idx) a.out_idx[i] = (int64_t)(uint32_t)(~(uint32_t)v);
+    }
+    return;
+  }
+  // large k: multi-CTA stable LSD radix sort of (~key << 32 | index)
+  for (uint64_t i = g; i < a.k; i += G) {
+    uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i));
+    a.sort_buf[0][i] = ((uint64_t)(~e.x) << 32) | (uint64_t)e.y;
+  }
+  if (!grid_barrier(gb)) return;
+  bool ok = true;
+  uint64_t* res = grid_lsd_sort(a, a.sort_buf[0], a.sort_buf[1], a.k, s_hist, ok);
+  if (!ok) return;
+  for (uint64_t i = g; i < a.k; i += G) {
+    const uint64_t v = ld_cg_u64(res + i);
+    if (a.out_vals) a.out_vals[i] = from_key(~(uint32_t)(v >> 32), a.km);
+    if (a.out_idx) a.out_idx[i] = (int64_t)(uint32_t)v;
+  }
+}
+
+}  // namespace drtopk

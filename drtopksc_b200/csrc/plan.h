@@ -1,0 +1,50 @@
+// plan.h -- host-side plan of one select: chosen path/parameters and the
+// workspace layout (byte offsets into one device allocation).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/drtopk.h"
+
+namespace drtopk {
+
+// control block words (zeroed by one memset per call)
+enum CtrlWord : int {
+  CW_ERR = 0,
+  CW_BAR_COUNT = 1,
+  CW_BAR_GEN = 2,
+  CW_DEL_MINMAX = 4,   // 2 words
+  CW_CAND_MINMAX = 6,  // 2 words
+  CW_CAND_COUNT = 8,
+  CW_STATS = 16,       // 32 words
+  CTRL_HDR_WORDS = 48
+};
+
+// stats slots >= 16 hold 64-bit %globaltimer stamps (lo, hi)
+enum StatTime : int { ST_T0 = 16, ST_T1 = 18, ST_T2 = 20, ST_T3 = 22 };
+
+struct Plan {
+  uint64_t n, k;
+  int km, algo, path, bucket, nbits, nb, alpha;
+  uint64_t S, M;
+  int first_levels;
+  int has_pos;
+  int sorted;
+  uint64_t cand_cap;
+  int fused_grid, sample_grid;
+  size_t fused_smem;
+  size_t run_words;
+  size_t off_ctrl, ctrl_bytes;
+  size_t off_del, off_pos, off_Atop, off_Acbuf0, off_Acbuf1;
+  size_t off_cand, off_Ccbuf0, off_Ctop;
+  size_t off_sort0, off_sort1, off_sortcnt;
+  size_t ws_bytes;
+};
+
+drtopk_status_t make_plan(uint64_t n, uint64_t k, drtopk_dtype_t dtype, const drtopk_params_t* p, int sms,
+                          int fused_grid, Plan* P);
+void layout(Plan* P, bool want_idx);
+int ref_alpha(double log2n, double k);
+
+}  // namespace drtopk

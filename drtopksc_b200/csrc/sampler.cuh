@@ -1,0 +1,241 @@
+// sampler.cuh -- delegate max-sampling, the streaming pass of Dr.Top-k.
+//
+// Semantics (reference: baseline+filter+beta+shuffle/radixselect.cuh):
+//   beta=1  sampleMax (882-918): del[j] = max of subrange j = keys
+//           [j*2^alpha, (j+1)*2^alpha) clipped to n.
+//   beta=2  sampleMax_NoReduction_Beta2 (966-1041): del[2j] = Max,
+//           del[2j+1] = Second (multiset second largest; 0 for a one-key
+//           subrange, as the reference's Second=0 start gives).
+// The reference launches one warp per subrange (beta=1) or stages 256
+// subranges in padded shared memory (beta=2).  Here one kernel covers every
+// alpha >= 1: warps walk 512-key chunks with four 128-bit evict-first loads
+// per lane in flight, reduce inside the lane, then across the lanes that
+// share a subrange with xor shuffles; small-subrange delegates are staged in
+// shared memory so they leave as coalesced stores.  The same pass builds the
+// histogram of the delegates' top digit (the first level of the first
+// select) or, for bucket select, their min/max, so no extra pass over the
+// delegate vector is needed to start the first select.
+#pragma once
+
+#include "common.cuh"
+
+namespace drtopk {
+
+struct SampleArgs {
+  const uint32_t* keys;  // raw input (uint32 or float32 bits)
+  uint64_t n;
+  int alpha;             // log2 subrange size, >= 1
+  int nbits;             // digit width for the fused histogram
+  int hmode;             // 0 none, 1 top-digit histogram, 2 min/max
+  int vec_ok;            // keys 16-byte aligned
+  uint32_t* del;         // beta=1: [M]; beta=2: [2M] interleaved (Max, Second)
+  uint16_t* pos;         // beta=2 with positions: offset of Max inside subrange j
+  uint32_t* hist;        // [1<<nbits] (hmode 1)
+  uint32_t* minmax;      // [2]: [0] = max(~v) (so min = ~[0]), [1] = max(v) (hmode 2)
+};
+
+constexpr int SAMPLE_THREADS = 256;
+constexpr int SAMPLE_WARPS = SAMPLE_THREADS / 32;
+
+// lane-local accumulator: first, second (beta=2), position of first
+struct Acc {
+  uint32_t a1, a2, p1;
+};
+
+template <int BETA, bool POS>
+DRTOPK_DEV void acc_push(Acc& s, uint32_t k, uint32_t p) {
+  if (BETA == 2) {
+    if (POS && k > s.a1) s.p1 = p;
+    top2_push(s.a1, s.a2, k);
+  } else {
+    s.a1 = max(s.a1, k);
+  }
+}
+
+template <int BETA, bool POS>
+DRTOPK_DEV void acc_merge(Acc& s, const Acc& o) {
+  if (BETA == 2) {
+    if (POS && (o.a1 > s.a1 || (o.a1 == s.a1 && o.p1 < s.p1))) s.p1 = o.p1;
+    top2_merge(s.a1, s.a2, o.a1, o.a2);
+  } else {
+    s.a1 = max(s.a1, o.a1);
+  }
+}
+
+template <int BETA, bool POS>
+DRTOPK_DEV Acc acc_shfl_xor(const Acc& s, int off) {
+  Acc o;
+  o.a1 = __shfl_xor_sync(0xffffffffu, s.a1, off);
+  o.a2 = BETA == 2 ? __shfl_xor_sync(0xffffffffu, s.a2, off) : 0u;
+  o.p1 = POS ? __shfl_xor_sync(0xffffffffu, s.p1, off) : 0u;
+  return o;
+}
+
+template <int KM>
+DRTOPK_DEV void load_row4(const SampleArgs& a, uint64_t base, uint64_t pol, bool full, uint32_t (&k)[4]) {
+  // four consecutive keys [base, base+4); keys >= n read as 0 (the max identity)
+  if (full) {
+    uint4 v = ld_stream_v4(a.keys + base, pol);
+    k[0] = to_key<KM>(v.x); k[1] = to_key<KM>(v.y); k[2] = to_key<KM>(v.z); k[3] = to_key<KM>(v.w);
+  } else {
+#pragma unroll
+    for (int e = 0; e < 4; ++e) k[e] = (base + e < a.n) ? to_key<KM>(ld_stream_u32(a.keys + base + e, pol)) : 0u;
+  }
+}
+
+template <int KM, int BETA, bool POS>
+__global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
+  __shared__ uint32_t s_hist[256];
+  __shared__ uint32_t s_stage[SAMPLE_WARPS][256 * BETA];
+  __shared__ uint16_t s_pstage[SAMPLE_WARPS][POS ? 256 : 1];
+  __shared__ uint32_t s_mm[2];
+
+  const int tid = threadIdx.x;
+  const unsigned lane = tid & 31u;
+  const int wib = tid >> 5;
+  const int nb = 1 << a.nbits;
+  const int dshift = 32 - a.nbits;
+  if (a.hmode == 1)
+    for (int i = tid; i < nb; i += SAMPLE_THREADS) s_hist[i] = 0;
+  if (tid < 2) s_mm[tid] = 0;
+  __syncthreads();
+
+  const uint64_t pol = make_evict_first_policy();
+  const int alpha = a.alpha;
+  const uint64_t S = 1ull << alpha;
+  const uint64_t M = (a.n + S - 1) >> alpha;
+  const uint64_t gwarp = (uint64_t)blockIdx.x * SAMPLE_WARPS + wib;
+  const uint64_t nwarps = (uint64_t)gridDim.x * SAMPLE_WARPS;
+  uint32_t mm_lo = 0, mm_hi = 0;  // lane-local max(~v), max(v) of emitted delegates
+
+  auto emit_hist = [&](uint32_t v) {
+    if (a.hmode == 1) atomicAdd(&s_hist[v >> dshift], 1u);
+    else if (a.hmode == 2) { mm_lo = max(mm_lo, ~v); mm_hi = max(mm_hi, v); }
+  };
+
+  if (alpha >= 9) {
+    // ---- one warp per subrange, 512-key chunks
+    for (uint64_t j = gwarp; j < M; j += nwarps) {
+      const uint64_t b = j << alpha;
+      const uint64_t e = min(a.n, b + S);
+      Acc s = {0u, 0u, 0u};
+      for (uint64_t c = b; c < e; c += 512) {
+        const bool full = a.vec_ok && (c + 512 <= e);
+        uint32_t k[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) load_row4<KM>(a, c + r * 128 + lane * 4, pol, full, k[r]);
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc_push<BETA, POS>(s, k[r][q], (uint32_t)(c - b) + r * 128 + lane * 4 + q);
+      }
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) acc_merge<BETA, POS>(s, acc_shfl_xor<BETA, POS>(s, off));
+      if (lane == 0) {
+        if (BETA == 2) {
+          *reinterpret_cast<uint2*>(a.del + 2 * j) = make_uint2(s.a1, s.a2);
+          if (POS) a.pos[j] = (uint16_t)s.p1;
+          emit_hist(s.a1);
+          emit_hist(s.a2);
+        } else {
+          a.del[j] = s.a1;
+          emit_hist(s.a1);
+        }
+      }
+    }
+  } else {
+    // ---- 512-key chunks holding 512/S subranges; lanes of a subrange:
+    // G = min(32, S/4) lanes per row, R = max(1, S/128) rows per subrange.
+    const uint64_t nchunks = (a.n + 511) >> 9;
+    const int G = alpha >= 7 ? 32 : (alpha >= 2 ? (1 << (alpha - 2)) : 1);
+    const int R = alpha >= 7 ? (1 << (alpha - 7)) : 1;
+    const int dpc = 512 >> alpha;  // delegates per chunk
+    uint32_t* stage = s_stage[wib];
+    for (uint64_t ch = gwarp; ch < nchunks; ch += nwarps) {
+      const uint64_t cb = ch << 9;
+      const bool full = a.vec_ok && (cb + 512 <= a.n);
+      uint32_t k[4][4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) load_row4<KM>(a, cb + r * 128 + lane * 4, pol, full, k[r]);
+      if (alpha == 1) {
+        // two 2-key subranges per lane per row
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int d = r * 64 + lane * 2 + h;
+            uint32_t x0 = k[r][2 * h], x1 = k[r][2 * h + 1];
+            if (BETA == 2) {
+              stage[2 * d] = max(x0, x1);
+              stage[2 * d + 1] = min(x0, x1);
+              if (POS) s_pstage[wib][d] = (x1 > x0) ? 1 : 0;
+            } else {
+              stage[d] = max(x0, x1);
+            }
+          }
+      } else {
+        Acc row[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          row[r] = {0u, 0u, 0u};
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc_push<BETA, POS>(row[r], k[r][q], (uint32_t)(r * 128 + lane * 4 + q));
+        }
+        // combine rows of the same subrange (S = 256: rows {0,1},{2,3})
+        if (R == 2) {
+          acc_merge<BETA, POS>(row[0], row[1]);
+          acc_merge<BETA, POS>(row[2], row[3]);
+          row[1] = row[2];
+        }
+        const int ngroups = 4 / R;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          if (r < ngroups) {
+            for (int off = 1; off < G; off <<= 1) acc_merge<BETA, POS>(row[r], acc_shfl_xor<BETA, POS>(row[r], off));
+            if ((lane & (G - 1)) == 0) {
+              const int d = r * (32 / G) + lane / G;
+              if (BETA == 2) {
+                stage[2 * d] = row[r].a1;
+                stage[2 * d + 1] = row[r].a2;
+                if (POS) s_pstage[wib][d] = (uint16_t)(row[r].p1 & (S - 1));
+              } else {
+                stage[d] = row[r].a1;
+              }
+            }
+          }
+        }
+      }
+      __syncwarp();
+      // coalesced copy-out of this chunk's delegates (skip subranges >= M)
+      const uint64_t d0 = ch * (uint64_t)dpc;
+      const int nd = (int)min((uint64_t)dpc, M - d0);
+      for (int i = lane; i < nd * BETA; i += 32) {
+        uint32_t v = stage[i];
+        a.del[d0 * BETA + i] = v;
+        emit_hist(v);
+      }
+      if (POS)
+        for (int i = lane; i < nd; i += 32) a.pos[d0 + i] = s_pstage[wib][i];
+      __syncwarp();
+    }
+  }
+
+  if (a.hmode == 2) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      mm_lo = max(mm_lo, __shfl_xor_sync(0xffffffffu, mm_lo, off));
+      mm_hi = max(mm_hi, __shfl_xor_sync(0xffffffffu, mm_hi, off));
+    }
+    if (lane == 0) { atomicMax(&s_mm[0], mm_lo); atomicMax(&s_mm[1], mm_hi); }
+  }
+  __syncthreads();
+  if (a.hmode == 1) {
+    for (int i = tid; i < nb; i += SAMPLE_THREADS)
+      if (s_hist[i]) atomicAdd(&a.hist[i], s_hist[i]);
+  } else if (a.hmode == 2 && tid == 0) {
+    atomicMax(&a.minmax[0], s_mm[0]);
+    atomicMax(&a.minmax[1], s_mm[1]);
+  }
+}
+
+}  // namespace drtopk

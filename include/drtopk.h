@@ -1,0 +1,238 @@
+/* drtopk.h -- C ABI of the B200-native Dr.Top-k selection library
+ * (libdrtopk.so).
+ *
+ * Plain C types only (device pointers as void*, CUDA streams as void*), so
+ * ctypes/cffi/JNI/cgo can bind it without CUDA headers.  All device pointers
+ * must belong to the handle's device.  Every call is stream-ordered and
+ * returns a status; nothing calls exit().  Results are exact: the k-th
+ * largest key equals ascending_sorted[n-k] (the reference's Enabletest check,
+ * baseline+filter+beta+shuffle/main.cu:281-296), and the top-k list is every
+ * key above it plus the lowest-index copies of it.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   baseline+filter+beta+shuffle/radixselect.cuh:1782-1784 sample_radix_select
+ *   baseline+filter+beta+shuffle/radixselect.cuh:1472      radix_select
+ *   bucket_select/bucketselect_combined.cuh:1279-1280      sample_bucket_select
+ *   bitonic/bitonic_com.cuh:609,668                        bitonic_firstTopk / bitonic
+ *   baseline+filter+beta+shuffle/main.cu:56-323            the topk.bin CLI (see topk_cli.cpp)
+ */
+#ifndef DRTOPK_H
+#define DRTOPK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DRTOPK_API __attribute__((visibility("default")))
+#else
+#define DRTOPK_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DRTOPK_OK = 0,
+  DRTOPK_EINVAL = 1,       /* invalid argument (k<1, k>n, bad nbits/alpha/...) */
+  DRTOPK_ENOMEM = 2,       /* device allocation failed or caller workspace too small */
+  DRTOPK_ECUDA = 3,        /* CUDA runtime error */
+  DRTOPK_EDEVICE = 4,      /* device-side check failed (see drtopk_sync_check) */
+  DRTOPK_EBUDGET = 5,      /* request exceeds the handle's / server's HBM budget */
+  DRTOPK_EUNSUPPORTED = 6, /* valid request outside this build's limits */
+  DRTOPK_ETIMEOUT = 7,     /* a bounded device wait gave up */
+  DRTOPK_EAGAIN = 8,       /* server: nothing finished yet / queue full */
+  DRTOPK_ECANCELLED = 9    /* server: request cancelled */
+} drtopk_status_t;
+
+typedef enum { DRTOPK_U32 = 0, DRTOPK_F32 = 1 } drtopk_dtype_t;
+
+typedef enum {
+  DRTOPK_ALGO_RADIX = 0,       /* Dr.Top-k radix (the reference's final version) */
+  DRTOPK_ALGO_BUCKET = 1,      /* Dr.Top-k bucket select (integer-exact buckets) */
+  DRTOPK_ALGO_BITONIC = 2,     /* Dr.Top-k bitonic top-k (k a power of two, k <= 2048) */
+  DRTOPK_ALGO_PLAIN_RADIX = 3, /* radix select without delegates (reference alpha==0) */
+  DRTOPK_ALGO_AUTO = 4         /* autotuner picks algorithm and parameters */
+} drtopk_algo_t;
+
+typedef struct {
+  int nbits;        /* bits per radix digit: 1,2,4,8 (reference NBitsPerDigit; default 8) */
+  int alpha;        /* log2 subrange size; -1: reference formula (main.cu:83); -2: autotuner */
+  int beta;         /* delegates per subrange on the small-alpha path; only 2 is valid (default 2) */
+  int path;         /* 0: reference rule (alpha>5 -> one delegate, else beta delegates); 1: one; 2: beta */
+  int algo;         /* drtopk_algo_t (default RADIX) */
+  int num_bucket;   /* bucket variant: buckets per level, 2..4096 (default 256) */
+  int largest;      /* 1: k largest (reference semantics, default); 0: k smallest */
+  int sorted;       /* 1: top-k sorted by key (best first), ties by index ascending */
+  int first_digits; /* beta path: digits used by the first select; 0: reference (32/nbits-3) */
+} drtopk_params_t;
+
+typedef struct {
+  int alpha;                 /* subrange size used: 2^alpha */
+  int beta;                  /* delegates per subrange used (1 or 2) */
+  int algo;                  /* algorithm actually run */
+  uint32_t first_threshold;  /* threshold from the first select (mapped key space) */
+  uint64_t n_subranges;      /* delegate subranges */
+  uint64_t n_selected;       /* subranges whose keys were concatenated */
+  uint64_t n_lonely;         /* single keys taken from subranges with one qualifying delegate */
+  uint64_t n_candidates;     /* size of the concatenated candidate vector */
+  int levels_first;          /* select levels run on the delegates */
+  int levels_second;         /* select levels run on the candidates */
+  uint32_t device_error;     /* device error word (0 = none) */
+  double ms_sample;          /* stage times of the last call (device clock) */
+  double ms_first;
+  double ms_concat;
+  double ms_second;
+  double ms_total;
+} drtopk_stats_t;
+
+typedef struct drtopk_handle* drtopk_handle_t;
+
+DRTOPK_API void drtopk_params_default(drtopk_params_t* p);
+DRTOPK_API const char* drtopk_status_str(drtopk_status_t s);
+
+/* A handle owns a resident device workspace (grown on demand, capped by
+ * hbm_budget_bytes; 0 = no cap), stage timers and the device error word.
+ * One handle serves one host thread at a time. */
+DRTOPK_API drtopk_status_t drtopk_create(drtopk_handle_t* h, int device, size_t hbm_budget_bytes);
+DRTOPK_API drtopk_status_t drtopk_destroy(drtopk_handle_t h);
+
+/* Scratch bytes a select of (n, k, dtype, params) needs -- replaces the
+ * caller-sized scratch of main.cu:205-250. */
+DRTOPK_API drtopk_status_t drtopk_workspace_size(uint64_t n, uint64_t k, drtopk_dtype_t dtype, const drtopk_params_t* p,
+                                      size_t* bytes);
+
+/* Exact top-k of d_keys[0..n) (uint32 or float32).  Outputs (device, any may
+ * be NULL): d_kth[1] the k-th key (same dtype as the input), d_vals[k] the
+ * top-k keys, d_idx[k] their indices.  n < 2^32, 1 <= k <= n. */
+DRTOPK_API drtopk_status_t drtopk_select(drtopk_handle_t h, const void* d_keys, drtopk_dtype_t dtype, uint64_t n, uint64_t k,
+                              const drtopk_params_t* p, void* d_kth, void* d_vals, int64_t* d_idx, void* stream);
+
+/* Same, with caller-owned scratch of at least drtopk_workspace_size bytes
+ * (256-byte aligned); the handle's own workspace is not touched. */
+DRTOPK_API drtopk_status_t drtopk_select_ws(drtopk_handle_t h, const void* d_keys, drtopk_dtype_t dtype, uint64_t n,
+                                 uint64_t k, const drtopk_params_t* p, void* d_kth, void* d_vals, int64_t* d_idx,
+                                 void* d_workspace, size_t workspace_bytes, void* stream);
+
+/* Synchronise the stream and report device-side failures of the last call
+ * (bounded waits that gave up, internal checks). */
+DRTOPK_API drtopk_status_t drtopk_sync_check(drtopk_handle_t h, void* stream);
+
+/* Statistics and stage times of the handle's last select (synchronises). */
+DRTOPK_API drtopk_status_t drtopk_last_stats(drtopk_handle_t h, drtopk_stats_t* st);
+
+/* Per-call kernel timing: between profile_begin and profile_end every select
+ * on this handle records CUDA events on its stream around the sampler and
+ * the fused kernel (up to max_calls calls).  profile_end synchronises and
+ * returns the summed device times (ms) of the two kernels and the number of
+ * calls recorded. */
+DRTOPK_API drtopk_status_t drtopk_profile_begin(drtopk_handle_t h, int max_calls);
+DRTOPK_API drtopk_status_t drtopk_profile_end(drtopk_handle_t h, double* ms_sample, double* ms_fused, int* ncalls);
+
+/* Parameters the autotuner picks for (n, k, dtype); p is updated in place. */
+DRTOPK_API drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_t dtype, drtopk_params_t* p);
+
+/* ---------------------------------------------------------------------
+ * Reference-compatible entry points (same arguments, same meaning,
+ * blocking like the reference; launch-shape arguments of the reference's
+ * own kernels are accepted and ignored; status instead of exit()).
+ * ------------------------------------------------------------------- */
+
+/* baseline+filter+beta+shuffle/radixselect.cuh:1782-1784 sample_radix_select.
+ * Max_d (NSubranges*beta keys) receives the delegates; *CountSelectedSubrange_d,
+ * *CountLonelyElements_d and *write_pos_d receive the number of selected
+ * subranges, lonely elements and candidates (the reference's counters).
+ * Stage times are returned in seconds like the reference's wtime() deltas. */
+DRTOPK_API drtopk_status_t drtopk_sample_radix_select(
+    uint32_t* vec_d, int num_element, int k, int num_bucket, uint32_t* TopKElement, int NBitsperDigit,
+    int CurrentDigit, int NSubranges, int SubRangesize, int alpha, double* timeforMaxsample,
+    double* timeforFirstTopK, double* timeForsecondTopK, double* timeforConcatenation, uint32_t* Max_d,
+    int* SubrangeId_d, int NSharedMemoryElements, int SizeOfSubWarp, int pow_size_Subwarp, int NSubWarps_InBlock,
+    int NSubRangesPerBlock, int NElementsPerBlock_ReadFromGlobal, int TotalBlocksrequired, int SizeOfAllocation,
+    int NThreadsPerBlock, int beta, int defaultContribution, int NthreadstoworkInreduction,
+    int* SelectedSubrangeId_d, int* CountLonelyElements_d, int* write_pos_d, uint32_t* ConcatenatedRange_d,
+    int* CountSelectedSubrange_d);
+
+/* baseline+filter+beta+shuffle/radixselect.cuh:1472 radix_select (no delegates). */
+DRTOPK_API drtopk_status_t drtopk_radix_select(uint32_t* vec_d, int num_element, int k, int num_bucket, uint32_t* TopKElement,
+                                    int NBitsperDigit, int CurrentDigit);
+
+/* bucket_select/bucketselect_combined.cuh:1279-1280 sample_bucket_select
+ * (k is the k of the k-th largest, as at bucket_select/main.cu:166). */
+DRTOPK_API drtopk_status_t drtopk_sample_bucket_select(
+    uint32_t* vec_d, int num_element, int k, int num_bucket, uint32_t* TopKElement, int NSubranges,
+    int SubRangesize, int alpha, double* timeforMaxsample, double* timeforFirstTopK, double* timeForsecondTopK,
+    double* timeforConcatenation, uint32_t* Max_d, int* SubrangeId_d, int beta, int defaultContribution,
+    int NthreadstoworkInreduction, int NThreadsPerBlock, int SizeOfAllocation, int NSharedMemoryElements,
+    int* SelectedSubrangeId_d, int* CountSelectedSubrange_d, int* CountLonelyElements_d, int* write_pos_d,
+    uint32_t* ConcatenatedRange_d);
+
+/* bitonic/sampleBitonic.cu:192 + bitonic_com.cuh:609-728: Dr.Top-k bitonic
+ * top-k of A_d[0..N) with subranges of 2^alpha keys (NormalBitonic=1: no
+ * delegates).  Writes the k largest keys sorted descending to d_topk (device)
+ * and, if d_idx is not NULL, their indices.  k must be a power of two <= 2048
+ * and N>>alpha >= k (sampleBitonic.cu:198-221). */
+DRTOPK_API drtopk_status_t drtopk_bitonic_topk(const uint32_t* A_d, int N, int k, int alpha, int NormalBitonic,
+                                    uint32_t* d_topk, int64_t* d_idx, uint32_t* TopKElement);
+
+/* ---------------------------------------------------------------------
+ * Batched form: many independent top-k problems in one persistent launch.
+ * Segment s covers keys[offsets[s] .. offsets[s+1]) of one dtype; its k is
+ * ks[s].  Outputs are packed at out_offsets[s] (exclusive scan of ks).
+ * All arrays are device arrays except where noted.
+ * ------------------------------------------------------------------- */
+typedef struct drtopk_batch* drtopk_batch_t;
+
+DRTOPK_API drtopk_status_t drtopk_batch_create(drtopk_batch_t* b, int device);
+DRTOPK_API drtopk_status_t drtopk_batch_destroy(drtopk_batch_t b);
+/* Plan a batch (host arrays h_offsets[nseg+1], h_ks[nseg], h_dtypes[nseg]):
+ * autotunes per segment and sizes the resident workspace.  Re-plan only
+ * when the segment layout changes; run() can then be graph-replayed. */
+DRTOPK_API drtopk_status_t drtopk_batch_plan(drtopk_batch_t b, int nseg, const uint64_t* h_offsets, const uint32_t* h_ks,
+                                  const int* h_dtypes, int sorted);
+DRTOPK_API drtopk_status_t drtopk_batch_run(drtopk_batch_t b, const void* d_keys, void* d_kth, void* d_vals, int64_t* d_idx,
+                                 void* stream);
+/* Capture run() into a CUDA graph once and replay it (same pointers). */
+DRTOPK_API drtopk_status_t drtopk_batch_run_graph(drtopk_batch_t b, const void* d_keys, void* d_kth, void* d_vals,
+                                       int64_t* d_idx, void* stream);
+DRTOPK_API drtopk_status_t drtopk_batch_sync_check(drtopk_batch_t b, void* stream);
+/* Per-segment choice of the autotuner: h_algo[nseg], h_alpha[nseg] (host). */
+DRTOPK_API drtopk_status_t drtopk_batch_describe(drtopk_batch_t b, int* h_algo, int* h_alpha, int* h_beta);
+
+/* ---------------------------------------------------------------------
+ * Served form: continuous batching of top-k requests under an HBM budget.
+ * Requests carry host keys; the server copies them into resident device
+ * buffers, admits them when budget and slots allow, runs admitted requests
+ * together, and returns exact results.
+ * ------------------------------------------------------------------- */
+typedef struct drtopk_server* drtopk_server_t;
+
+typedef struct {
+  uint64_t id;          /* request id returned by submit */
+  int status;           /* drtopk_status_t of this request */
+  uint32_t kth;         /* k-th key (raw bits of the request dtype) */
+  double t_submit_ms;   /* server clock (ms since creation) */
+  double t_start_ms;
+  double t_done_ms;
+} drtopk_result_t;
+
+DRTOPK_API drtopk_status_t drtopk_server_create(drtopk_server_t* s, int device, size_t hbm_budget_bytes, int max_inflight);
+DRTOPK_API drtopk_status_t drtopk_server_destroy(drtopk_server_t s);
+/* Submit a request (keys are copied before return).  out_vals / out_idx are
+ * host buffers of k entries, filled when the request completes (may be NULL). */
+DRTOPK_API drtopk_status_t drtopk_server_submit(drtopk_server_t s, const void* h_keys, drtopk_dtype_t dtype, uint64_t n,
+                                     uint64_t k, int sorted, void* out_vals, int64_t* out_idx, uint64_t* id);
+/* Pop up to max finished results; *count receives how many. */
+DRTOPK_API drtopk_status_t drtopk_server_poll(drtopk_server_t s, drtopk_result_t* results, int max, int* count);
+/* Cancel a request that has not started. */
+DRTOPK_API drtopk_status_t drtopk_server_cancel(drtopk_server_t s, uint64_t id);
+/* Block until every submitted request has finished (bounded by timeout_ms; -1 = no bound). */
+DRTOPK_API drtopk_status_t drtopk_server_drain(drtopk_server_t s, int timeout_ms);
+/* Current resident bytes and in-flight request count. */
+DRTOPK_API drtopk_status_t drtopk_server_usage(drtopk_server_t s, size_t* resident_bytes, int* inflight, int* queued);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRTOPK_H */
