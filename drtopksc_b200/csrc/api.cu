@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/drtopk.h"
+#include "bitonic.cuh"
 #include "fused.cuh"
 #include "plan.h"
 #include "sampler.cuh"
@@ -78,6 +79,35 @@ static cudaError_t fused_max_grid(DevInfo* d, int km, size_t smem, int* grid) {
   return cudaSuccess;
 }
 
+template <int KM>
+static void* bitonic_fn() {
+  return (void*)k_bitonic<KM>;
+}
+static void* bitonic_ptr(int km) {
+  switch (km) {
+    case KM_U32: return bitonic_fn<KM_U32>();
+    case KM_F32: return bitonic_fn<KM_F32>();
+    case KM_U32_MIN: return bitonic_fn<KM_U32_MIN>();
+    default: return bitonic_fn<KM_F32_MIN>();
+  }
+}
+
+static cudaError_t bitonic_max_grid(DevInfo* d, int km, size_t smem, int* grid) {
+  static int occ_cache[64][4];
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  int& occ = occ_cache[d->device][km];
+  if (occ == 0) {
+    cudaError_t e = cudaFuncSetAttribute(bitonic_ptr(km), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int o = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, bitonic_ptr(km), FUSED_THREADS, smem);
+    if (e != cudaSuccess) return e;
+    occ = std::max(1, o);
+  }
+  *grid = occ * d->sms;
+  return cudaSuccess;
+}
+
 // ------------------------------------------------------------ planning
 static inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -100,8 +130,9 @@ drtopk_status_t make_plan(uint64_t n, uint64_t k, drtopk_dtype_t dtype, const dr
     drtopk_status_t s = drtopk_autotune(n, k, dtype, &p);
     if (s != DRTOPK_OK) return s;
   }
-  if (p.algo != DRTOPK_ALGO_RADIX && p.algo != DRTOPK_ALGO_BUCKET && p.algo != DRTOPK_ALGO_PLAIN_RADIX)
-    return DRTOPK_EUNSUPPORTED;  // bitonic has its own entry point
+  if (p.algo != DRTOPK_ALGO_RADIX && p.algo != DRTOPK_ALGO_BUCKET && p.algo != DRTOPK_ALGO_PLAIN_RADIX &&
+      p.algo != DRTOPK_ALGO_BITONIC)
+    return DRTOPK_EINVAL;
   P->n = n;
   P->k = k;
   P->km = (dtype == DRTOPK_F32 ? 1 : 0) + (p.largest ? 0 : 2);
@@ -116,6 +147,30 @@ drtopk_status_t make_plan(uint64_t n, uint64_t k, drtopk_dtype_t dtype, const dr
   }
   P->sorted = p.sorted;
   const double log2n = std::log2((double)n);
+  if (p.algo == DRTOPK_ALGO_BITONIC) {
+    // bitonic/sampleBitonic.cu:198-221: k a power of two, NSubranges >= k;
+    // the shared-memory network bounds k (bitonic_com.cuh:619-637)
+    if ((k & (k - 1)) != 0 || k > (uint64_t)BITONIC_MAX_K) return DRTOPK_EINVAL;
+    P->path = PATH_BITONIC;
+    P->sorted = 1;
+    int alpha = p.alpha;
+    if (alpha < 0) {
+      alpha = ref_alpha(log2n, (double)k);
+      while (alpha > 2 && ((n + (1ull << alpha) - 1) >> alpha) < k) alpha--;
+    }
+    if (alpha == 0 || p.path == 3) {
+      P->normal = 1;
+      P->alpha = 0;
+    } else {
+      if (alpha < 2 || alpha > 24) return DRTOPK_EINVAL;
+      P->alpha = alpha;
+      P->S = 1ull << alpha;
+      P->M = (n + P->S - 1) >> alpha;
+      if (P->M < k) return DRTOPK_EINVAL;
+    }
+    P->fused_grid = fused_grid;
+    return DRTOPK_OK;
+  }
   int alpha = p.alpha;
   const bool auto_alpha = alpha < 0;
   if (auto_alpha) {
@@ -176,6 +231,19 @@ void layout(Plan* P, bool want_idx) {
   P->off_ctrl = take(ctrl_words * 4);
   P->ctrl_bytes = ctrl_words * 4;
   uint64_t ncand_cap = 0;
+  if (P->path == PATH_BITONIC) {
+    const uint64_t T = BITONIC_TILE;
+    uint64_t cap;
+    if (P->normal) cap = (P->n + T - 1) / T * k;
+    else cap = std::max<uint64_t>((P->M + T - 1) / T * k, k * P->S);
+    cap = std::max<uint64_t>(cap, T);
+    P->bbuf_cap = cap;
+    if (!P->normal) P->off_del = take(P->M * 4);
+    P->off_bbuf0 = take(cap * 8);
+    P->off_bbuf1 = take(cap * 8);
+    P->ws_bytes = off;
+    return;
+  }
   if (P->path == PATH_DEFAULT) {
     P->off_del = take(P->M * 4);
     P->off_Atop = take(k * 8);
@@ -294,15 +362,18 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
     while (np2 < k) np2 <<= 1;
     smem = std::max(smem, np2 * 8);
   }
+  if (P->path == PATH_BITONIC) smem = (size_t)BITONIC_TILE * 8;
   P->fused_smem = smem;
   int maxgrid = 0;
-  if (fused_max_grid(di, P->km, smem, &maxgrid) != cudaSuccess) return DRTOPK_ECUDA;
+  if ((P->path == PATH_BITONIC ? bitonic_max_grid(di, P->km, smem, &maxgrid)
+                                : fused_max_grid(di, P->km, smem, &maxgrid)) != cudaSuccess)
+    return DRTOPK_ECUDA;
   // grid: the whole GPU for large inputs, fewer CTAs for small ones (fewer
   // barrier participants)
   uint64_t want = std::max<uint64_t>((uint64_t)di->sms / 2, n >> 15);
   P->fused_grid = (int)std::min<uint64_t>((uint64_t)maxgrid, std::max<uint64_t>(1, want));
   // sampler grid: persistent, capped by the work items
-  if (P->path != PATH_PLAIN) {
+  if (P->path != PATH_PLAIN && !(P->path == PATH_BITONIC && P->normal)) {
     uint64_t items = P->alpha >= 9 ? P->M : ((n + 511) >> 9);
     uint64_t ctas = (items + SAMPLE_WARPS - 1) / SAMPLE_WARPS;
     P->sample_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(ctas, (uint64_t)di->sms * di->occ_sample));
@@ -365,12 +436,83 @@ static RunBufs run_bufs(char* ctrl, const Plan& P, int which) {
   return r;
 }
 
+static cudaError_t launch_sampler_km(const Plan& P, const SampleArgs& sa, int beta, cudaStream_t st) {
+  switch (P.km) {
+    case KM_U32: return launch_sample<KM_U32>(sa, beta, P.has_pos, P.sample_grid, st);
+    case KM_F32: return launch_sample<KM_F32>(sa, beta, P.has_pos, P.sample_grid, st);
+    case KM_U32_MIN: return launch_sample<KM_U32_MIN>(sa, beta, P.has_pos, P.sample_grid, st);
+    default: return launch_sample<KM_F32_MIN>(sa, beta, P.has_pos, P.sample_grid, st);
+  }
+}
+
+static drtopk_status_t launch_coop(void* fn, const Plan& P, void* argp, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P.fused_grid);
+  cfg.blockDim = dim3(FUSED_THREADS);
+  cfg.dynamicSmemBytes = P.fused_smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* args[] = {argp};
+  return cudaLaunchKernelExC(&cfg, fn, args) == cudaSuccess ? DRTOPK_OK : DRTOPK_ECUDA;
+}
+
+static drtopk_status_t enqueue_bitonic(const Plan& P, const void* d_keys, void* d_kth, void* d_vals, int64_t* d_idx,
+                                       char* ws, cudaStream_t st, cudaEvent_t* ev) {
+  char* ctrl = ws + P.off_ctrl;
+  uint32_t* cw = reinterpret_cast<uint32_t*>(ctrl);
+  const bool vec_ok = (reinterpret_cast<uintptr_t>(d_keys) & 15u) == 0;
+  BitonicArgs b;
+  std::memset(&b, 0, sizeof(b));
+  b.keys = static_cast<const uint32_t*>(d_keys);
+  b.n = P.n;
+  b.k = (uint32_t)P.k;
+  b.km = P.km;
+  b.alpha = P.alpha;
+  b.M = P.M;
+  b.normal = P.normal;
+  b.vec_ok = vec_ok;
+  b.del = P.normal ? nullptr : reinterpret_cast<const uint32_t*>(ws + P.off_del);
+  b.buf[0] = reinterpret_cast<uint64_t*>(ws + P.off_bbuf0);
+  b.buf[1] = reinterpret_cast<uint64_t*>(ws + P.off_bbuf1);
+  b.buf_cap = P.bbuf_cap;
+  b.cand_count = cw + CW_CAND_COUNT;
+  b.out_kth = static_cast<uint32_t*>(d_kth);
+  b.out_vals = static_cast<uint32_t*>(d_vals);
+  b.out_idx = d_idx;
+  b.stats = cw + CW_STATS;
+  b.gb.count = cw + CW_BAR_COUNT;
+  b.gb.gen = cw + CW_BAR_GEN;
+  b.gb.err = cw + CW_ERR;
+  b.gb.nblocks = (uint32_t)P.fused_grid;
+  if (!P.normal) {
+    SampleArgs sa;
+    std::memset(&sa, 0, sizeof(sa));
+    sa.keys = b.keys;
+    sa.n = P.n;
+    sa.alpha = P.alpha;
+    sa.nbits = 8;
+    sa.hmode = 0;
+    sa.vec_ok = vec_ok;
+    sa.del = const_cast<uint32_t*>(b.del);
+    if (launch_sampler_km(P, sa, 1, st) != cudaSuccess) return DRTOPK_ECUDA;
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  drtopk_status_t s = launch_coop(bitonic_ptr(P.km), P, &b, st);
+  if (ev) cudaEventRecord(ev[2], st);
+  return s;
+}
+
 drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, void* d_kth, void* d_vals,
                                int64_t* d_idx, char* ws, cudaStream_t st, cudaEvent_t* ev) {
   char* ctrl = ws + P.off_ctrl;
   uint32_t* cw = reinterpret_cast<uint32_t*>(ctrl);
   if (cudaMemsetAsync(ctrl, 0, P.ctrl_bytes, st) != cudaSuccess) return DRTOPK_ECUDA;
   if (ev) cudaEventRecord(ev[0], st);
+  if (P.path == PATH_BITONIC) return enqueue_bitonic(P, d_keys, d_kth, d_vals, d_idx, ws, st, ev);
   const bool vec_ok = (reinterpret_cast<uintptr_t>(d_keys) & 15u) == 0;
   FusedArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -437,31 +579,13 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
     sa.hist = a.A.H[0];
     sa.minmax = cw + CW_DEL_MINMAX;
     const int beta = P.path == PATH_BETA ? 2 : 1;
-    cudaError_t e;
-    switch (P.km) {
-      case KM_U32: e = launch_sample<KM_U32>(sa, beta, P.has_pos, P.sample_grid, st); break;
-      case KM_F32: e = launch_sample<KM_F32>(sa, beta, P.has_pos, P.sample_grid, st); break;
-      case KM_U32_MIN: e = launch_sample<KM_U32_MIN>(sa, beta, P.has_pos, P.sample_grid, st); break;
-      default: e = launch_sample<KM_F32_MIN>(sa, beta, P.has_pos, P.sample_grid, st); break;
-    }
-    if (e != cudaSuccess) return DRTOPK_ECUDA;
+    if (launch_sampler_km(P, sa, beta, st) != cudaSuccess) return DRTOPK_ECUDA;
   }
   if (ev) cudaEventRecord(ev[1], st);
   // ---- fused cooperative kernel
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(P.fused_grid);
-  cfg.blockDim = dim3(FUSED_THREADS);
-  cfg.dynamicSmemBytes = P.fused_smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  void* args[] = {&a};
-  if (cudaLaunchKernelExC(&cfg, fused_ptr(P.km), args) != cudaSuccess) return DRTOPK_ECUDA;
+  drtopk_status_t s = launch_coop(fused_ptr(P.km), P, &a, st);
   if (ev) cudaEventRecord(ev[2], st);
-  return DRTOPK_OK;
+  return s;
 }
 
 }  // namespace drtopk
@@ -790,4 +914,25 @@ extern "C" drtopk_status_t drtopk_sample_bucket_select(
   if (CountLonelyElements_d) cudaMemcpy(CountLonelyElements_d, &cnt[1], 4, cudaMemcpyHostToDevice);
   if (write_pos_d) cudaMemcpy(write_pos_d, &cnt[2], 4, cudaMemcpyHostToDevice);
   return DRTOPK_OK;
+}
+
+extern "C" drtopk_status_t drtopk_bitonic_topk(const uint32_t* A_d, int N, int k, int alpha, int NormalBitonic,
+                                               uint32_t* d_topk, int64_t* d_idx, uint32_t* TopKElement) {
+  if (!A_d || N <= 0 || k <= 0 || k > N) return DRTOPK_EINVAL;
+  drtopk_params_t p;
+  drtopk_params_default(&p);
+  p.algo = DRTOPK_ALGO_BITONIC;
+  p.alpha = NormalBitonic ? 0 : alpha;
+  p.path = NormalBitonic ? 3 : 0;
+  drtopk_handle_t h;
+  drtopk_status_t s = default_handle(&h);
+  if (s != DRTOPK_OK) return s;
+  uint32_t* d_kth = nullptr;
+  if (cudaMalloc(&d_kth, 4) != cudaSuccess) return DRTOPK_ENOMEM;
+  s = drtopk_select(h, A_d, DRTOPK_U32, (uint64_t)N, (uint64_t)k, &p, d_kth, d_topk, d_idx, nullptr);
+  if (s == DRTOPK_OK) s = drtopk_sync_check(h, nullptr);
+  if (s == DRTOPK_OK && TopKElement && cudaMemcpy(TopKElement, d_kth, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    s = DRTOPK_ECUDA;
+  cudaFree(d_kth);
+  return s;
 }

@@ -28,7 +28,7 @@
 
 namespace drtopk {
 
-enum Path : int { PATH_DEFAULT = 0, PATH_BETA = 1, PATH_PLAIN = 2 };
+enum Path : int { PATH_DEFAULT = 0, PATH_BETA = 1, PATH_PLAIN = 2, PATH_BITONIC = 3 };
 
 constexpr int SMALL_SORT = 4096;  // top-k sorted in one CTA's shared memory up to this k
 

@@ -2,7 +2,6 @@
 #include "../../include/drtopk.h"
 
 extern "C" {
-drtopk_status_t drtopk_bitonic_topk(const uint32_t*, int, int, int, int, uint32_t*, int64_t*, uint32_t*) { return DRTOPK_EUNSUPPORTED; }
 drtopk_status_t drtopk_batch_create(drtopk_batch_t* b, int) { if (b) *b = nullptr; return DRTOPK_EUNSUPPORTED; }
 drtopk_status_t drtopk_batch_destroy(drtopk_batch_t) { return DRTOPK_OK; }
 drtopk_status_t drtopk_batch_plan(drtopk_batch_t, int, const uint64_t*, const uint32_t*, const int*, int) { return DRTOPK_EUNSUPPORTED; }

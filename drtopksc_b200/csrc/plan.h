@@ -39,6 +39,10 @@ struct Plan {
   size_t off_del, off_pos, off_Atop, off_Acbuf0, off_Acbuf1;
   size_t off_cand, off_Ccbuf0, off_Ctop;
   size_t off_sort0, off_sort1, off_sortcnt;
+  // bitonic variant
+  int normal;  // NormalBitonic: no delegates
+  uint64_t bbuf_cap;
+  size_t off_bbuf0, off_bbuf1;
   size_t ws_bytes;
 };
 
