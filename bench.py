@@ -4,8 +4,9 @@
 Workload (the reference's headline config): N = 2^30
 uint32 keys (4 GiB) drawn uniform over [0, 2^32-1] (seeded Philox on the
 device -- synthetic data standing in for the reference's unseeded
-random_device draws), 8-bit digits, beta = 2, alpha from the reference
-formula, k swept over 2^0..2^24.  One step = one pass of the sweep: 25
+random_device draws), 8-bit digits, beta = 2, alpha (and path) per k from
+the autotuner (--alpha-mode ref: the reference's formula), k swept over
+2^0..2^24.  One step = one pass of the sweep: 25
 exact top-k calls (k-th value + the k largest values) over the resident
 keys.  metric: keys/s = 25 * N * steps / device time.
 
@@ -171,6 +172,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--alpha-mode", choices=["auto", "ref"], default="auto",
+                    help="auto: per-k parameters from the autotuner (headline); ref: the reference's alpha formula")
+    ap.add_argument("--no-table", action="store_true", help="skip the per-k tables after the timed region")
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -202,11 +206,14 @@ def main():
     h = D.Handle(local)
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream or None
-    p = D.params()  # reference defaults: 8-bit digits, beta=2, alpha formula
+    # 8-bit digits, beta=2; alpha (and path / threshold digits) per k from the
+    # autotuner, or the reference formula with --alpha-mode ref
+    p_ref = D.params()
+    plist = [D.autotune(n, k, D.U32, D.params(alpha=-2)) if args.alpha_mode == "auto" else p_ref for k in ks]
 
     def one_step():
         for i, k in enumerate(ks):
-            h.select_raw(keys.data_ptr(), D.U32, n, k, p, kth.data_ptr() + 4 * i, vals.data_ptr(), None, sp)
+            h.select_raw(keys.data_ptr(), D.U32, n, k, plist[i], kth.data_ptr() + 4 * i, vals.data_ptr(), None, sp)
 
     for _ in range(args.warmup):
         one_step()
@@ -257,26 +264,35 @@ def main():
     if traffic and traffic.get("n") and traffic.get("dram_bytes_per_launch"):
         traffic_bytes = traffic["dram_bytes_per_launch"] * (n / traffic["n"])
 
-    # ---------------- per-k table (short, after the timed region)
-    sweep = {}
-    for i, k in enumerate(ks):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = 3
-        a.record(stream)
-        for _ in range(reps):
-            h.select_raw(keys.data_ptr(), D.U32, n, k, p, kth.data_ptr() + 4 * i, vals.data_ptr(), None, sp)
-        b.record(stream)
-        torch.cuda.synchronize(dev)
-        kms = a.elapsed_time(b) / reps
-        st = h.stats()
-        row = {"ms": round(kms, 4), "keys_per_s": n / (kms * 1e-3),
-               "frac_of_measured_hbm": (4.0 * n + 4.0 * k) / (kms * 1e-3) / (peak * 1e9),
-               "alpha": st["alpha"], "beta": st["beta"], "candidates": st["n_candidates"],
-               "ms_sample": round(st["ms_sample"], 4)}
-        if k in REF_V100S_MS and n == 1 << 30:
-            row["reference_v100s_ms"] = REF_V100S_MS[k]
-        sweep[str(k)] = row
-    h.sync_check(stream)
+    # ---------------- per-k tables (short, after the timed region)
+    def table(params_for):
+        out = {}
+        for i, k in enumerate(ks):
+            pk = params_for(i, k)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = 3
+            a.record(stream)
+            for _ in range(reps):
+                h.select_raw(keys.data_ptr(), D.U32, n, k, pk, kth.data_ptr() + 4 * i, vals.data_ptr(), None, sp)
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            kms = a.elapsed_time(b) / reps
+            st = h.stats()
+            row = {"ms": round(kms, 4), "keys_per_s": n / (kms * 1e-3),
+                   "frac_of_measured_hbm": (4.0 * n + 4.0 * k) / (kms * 1e-3) / (peak * 1e9),
+                   "alpha": st["alpha"], "beta": st["beta"], "candidates": st["n_candidates"],
+                   "ms_sample": round(st["ms_sample"], 4)}
+            if k in REF_V100S_MS and n == 1 << 30:
+                row["reference_v100s_ms"] = REF_V100S_MS[k]
+            out[str(k)] = row
+        h.sync_check(stream)
+        return out
+
+    sweep, sweep_ref = {}, {}
+    if not args.no_table:
+        sweep = table(lambda i, k: plist[i])
+        if args.alpha_mode == "auto":
+            sweep_ref = table(lambda i, k: p_ref)
 
     # ---------------- end to end through the C ABI with host buffers
     e2e = None
@@ -295,7 +311,8 @@ def main():
         for _ in range(args.e2e_steps):
             for i, k in enumerate(ks):
                 dkeys.copy_(host, non_blocking=True)
-                h.select_raw(dkeys.data_ptr(), D.U32, n, k, p, kth.data_ptr() + 4 * i, vals.data_ptr(), None, sp)
+                h.select_raw(dkeys.data_ptr(), D.U32, n, k, plist[i], kth.data_ptr() + 4 * i, vals.data_ptr(), None,
+                             sp)
                 h_kth[i:i + 1].copy_(kth[i:i + 1], non_blocking=True)
                 h_vals[:k].copy_(vals[:k], non_blocking=True)
                 d2h += 4 + 4 * k
@@ -331,7 +348,8 @@ def main():
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32", "data": "synthetic (seeded torch Philox, uniform uint32 over [0, 2^32-1])",
             "config": {"workload": "Dr.Top-k radix, N=2^%d uint32 uniform, k=2^0..2^24 (one step = the sweep), "
-                                   "nbits=8, beta=2, alpha=reference formula" % args.log2n,
+                                   "nbits=8, beta=2, alpha per k: %s" % (args.log2n, "autotuner" if args.alpha_mode == "auto"
+                                                                          else "reference formula"),
                        "n": n, "ks": len(ks), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "input 4 GiB >> 126 MB L2 (no flush needed)"},
             "roofline": {"bound": "hbm", "kernel": "k_sample (delegate sampler)", "achieved": achieved,
@@ -345,6 +363,7 @@ def main():
             "e2e": e2e,
             "gpu_launches": 2 * calls,
             "k_sweep": sweep,
+            "k_sweep_reference_alpha": sweep_ref,
         }
         print(json.dumps(out), flush=True)
     h.close()

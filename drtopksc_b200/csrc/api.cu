@@ -253,6 +253,7 @@ void layout(Plan* P, bool want_idx) {
   } else if (P->path == PATH_BETA) {
     P->off_del = take(P->M * 8);
     if (P->has_pos) P->off_pos = take(P->M * 2);
+    P->off_sel = take(P->M * 4);
     ncand_cap = P->n;
   } else {
     ncand_cap = P->n;
@@ -534,6 +535,7 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
   a.C = run_bufs(ctrl, P, 2);
   a.CF = run_bufs(ctrl, P, 3);
   a.cand_count = cw + CW_CAND_COUNT;
+  a.sel_count = cw + CW_SEL_COUNT;
   a.cand_minmax = cw + CW_CAND_MINMAX;
   a.stats = cw + CW_STATS;
   a.sort_tot = cw + CTRL_HDR_WORDS + 4 * (size_t)P.run_words;
@@ -559,6 +561,7 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
     a.del = reinterpret_cast<const uint32_t*>(ws + P.off_del);
     a.has_pos = P.has_pos;
     if (P.has_pos) a.pos = reinterpret_cast<const uint16_t*>(ws + P.off_pos);
+    a.sel = reinterpret_cast<uint32_t*>(ws + P.off_sel);
   }
   if (P.sorted && P.k > (uint64_t)SMALL_SORT) {
     a.sort_buf[0] = reinterpret_cast<uint64_t*>(ws + P.off_sort0);
@@ -762,36 +765,79 @@ extern "C" drtopk_status_t drtopk_profile_end(drtopk_handle_t h, double* ms_samp
   return s;
 }
 
+// Traffic model of the delegate paths (bytes beyond the 4n streaming read),
+// for n keys, k wanted, subranges of S = 2^alpha keys (M = n/S), assuming
+// keys i.i.d. in rank (q = k/n is the fraction of top keys):
+//   one delegate (default path):  4M (write) + 4M (first select read)
+//                                 + 4kS (the k kept subranges re-read)
+//   two delegates (beta path):    8M (write) + 8M per extra threshold digit
+//                                 + 8M (filter read) + 4S per subrange with
+//                                 >= 2 keys above the threshold + 8 per
+//                                 candidate; a threshold of d digits admits
+//                                 an extra ~2^-8d of the keys (truncation).
+// Subrange counts per bucket follow Poisson(lambda = q' S).
+static double cost_default(double n, double k, double S) {
+  const double M = n / S;
+  return 8.0 * M + 4.0 * k * S + 24.0 * k;
+}
+static double cost_beta(double n, double k, double S, int digits) {
+  const double M = n / S;
+  const double q = k / n + std::ldexp(1.0, -8 * digits);
+  const double lam = q * S;
+  const double e = std::exp(-lam);
+  const double p_sel = 1.0 - e * (1.0 + lam);
+  const double p_lone = lam * e;
+  const double cand = M * p_lone + M * p_sel * (lam + 1.0);
+  return 16.0 * M + 8.0 * M * (digits - 1) + M * p_sel * 4.0 * S + 24.0 * cand;
+}
+
 extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_t dtype, drtopk_params_t* p) {
   if (!p || n == 0 || k < 1 || k > n) return DRTOPK_EINVAL;
   (void)dtype;
-  // Traffic model of the delegate path (bytes beyond the 4n streaming read):
-  //   one delegate per subrange: ~8n/S (write + first-select read) + 4kS
-  //   (the k kept subranges are re-read) -> minimum near S = sqrt(2n/k).
-  // Small segments (n <= 2^16) are cheaper as a plain select.
   if (p->algo == DRTOPK_ALGO_AUTO) p->algo = DRTOPK_ALGO_RADIX;
-  if (p->algo == DRTOPK_ALGO_BITONIC) return DRTOPK_OK;
+  if (p->algo == DRTOPK_ALGO_BITONIC) {
+    if (p->alpha < 0) {
+      int alpha = (int)std::lround(std::log2(std::sqrt(2.0 * (double)n / (double)k)));
+      alpha = std::max(2, std::min(alpha, 16));
+      while (alpha > 2 && (n >> alpha) < k) alpha--;
+      p->alpha = alpha;
+    }
+    return DRTOPK_OK;
+  }
+  // small inputs: the delegate pass does not pay for itself
   if (n <= (1ull << 16) && p->algo == DRTOPK_ALGO_RADIX) {
     p->algo = DRTOPK_ALGO_PLAIN_RADIX;
     p->alpha = 0;
     return DRTOPK_OK;
   }
-  double s = std::sqrt(2.0 * (double)n / (double)k);
-  int alpha = (int)std::lround(std::log2(std::max(1.0, s)));
-  // keep enough subranges (M >= 8k) so the first select has room to filter
-  while (alpha > 2 && ((n >> alpha) < 8 * k)) alpha--;
-  alpha = std::max(2, std::min(alpha, 16));
-  if (alpha >= 6 && (n >> alpha) >= k) {
-    p->alpha = alpha;
-    p->path = 1;
-  } else {
-    // large k relative to n: two delegates per subrange (beta path) with
-    // small subranges and a two-digit threshold (fewer lonely candidates)
-    alpha = std::max(2, std::min(5, alpha));
-    p->alpha = alpha;
-    p->path = 2;
+  const double dn = (double)n, dk = (double)k;
+  double best = 1e300;
+  int best_alpha = 0, best_path = 1, best_digits = 0;
+  for (int alpha = 2; alpha <= 16; ++alpha) {
+    const double S = std::ldexp(1.0, alpha);
+    const uint64_t M = (n + (1ull << alpha) - 1) >> alpha;
+    if (alpha >= 2 && M >= k) {
+      const double c = cost_default(dn, dk, S);
+      if (c < best) { best = c; best_alpha = alpha; best_path = 1; best_digits = 0; }
+    }
+    if (2 * M >= k && p->beta == 2) {
+      const int maxd = p->nbits == 8 ? 2 : 1;
+      for (int d = 1; d <= maxd; ++d) {
+        const double c = cost_beta(dn, dk, S, p->nbits == 8 ? d : (32 / p->nbits - 3));
+        if (c < best) { best = c; best_alpha = alpha; best_path = 2; best_digits = d; }
+      }
+    }
+  }
+  if (best_alpha == 0) {  // nothing fits (k close to n): plain select
+    p->algo = p->algo == DRTOPK_ALGO_BUCKET ? p->algo : DRTOPK_ALGO_PLAIN_RADIX;
+    p->alpha = 0;
+    return DRTOPK_OK;
+  }
+  p->alpha = best_alpha;
+  p->path = best_path;
+  if (best_path == 2) {
     p->beta = 2;
-    if (p->nbits == 8 && p->first_digits == 0) p->first_digits = 2;
+    if (p->nbits == 8) p->first_digits = best_digits;
   }
   return DRTOPK_OK;
 }

@@ -116,6 +116,80 @@ DRTOPK_DEV uint32_t warp_append(bool pred, uint32_t* counter) {
   return base + __popc(b & ((1u << lane) - 1u));
 }
 
+// Block-aggregated append to two lists: every thread of the block passes the
+// number of items it will write to list A and list B (each < 2^16 summed
+// over the block); one atomic per list per call; returns this thread's
+// first slot in each list.  Must be called by all threads of the block.
+struct Slots2 {
+  uint32_t a, b;
+};
+DRTOPK_DEV Slots2 block_append2(uint32_t ca, uint32_t cb, uint32_t* counter_a, uint32_t* counter_b) {
+  __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_base[2];
+  const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  uint32_t v = ca | (cb << 16);
+  uint32_t incl = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+    if ((int)lane >= off) incl += y;
+  }
+  if (lane == 31) s_warp[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t w = lane < nw ? s_warp[lane] : 0u;
+    uint32_t wi = w;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, wi, off);
+      if ((int)lane >= off) wi += y;
+    }
+    if (lane < nw) s_warp[lane] = wi - w;  // exclusive warp prefix
+    if (lane == 31) {
+      const uint32_t ta = wi & 0xffffu, tb = wi >> 16;
+      s_base[0] = ta ? atomicAdd(counter_a, ta) : 0u;
+      s_base[1] = tb ? atomicAdd(counter_b, tb) : 0u;
+    }
+  }
+  __syncthreads();
+  const uint32_t ex = s_warp[wid] + incl - v;
+  Slots2 r;
+  r.a = s_base[0] + (ex & 0xffffu);
+  r.b = s_base[1] + (ex >> 16);
+  __syncthreads();
+  return r;
+}
+
+// single-list variant with 32-bit counts
+DRTOPK_DEV uint32_t block_append1(uint32_t c, uint32_t* counter) {
+  __shared__ uint32_t s_warp1[32];
+  __shared__ uint32_t s_base1;
+  const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  uint32_t incl = c;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+    if ((int)lane >= off) incl += y;
+  }
+  if (lane == 31) s_warp1[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t w = lane < nw ? s_warp1[lane] : 0u;
+    uint32_t wi = w;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, wi, off);
+      if ((int)lane >= off) wi += y;
+    }
+    if (lane < nw) s_warp1[lane] = wi - w;
+    if (lane == 31) s_base1 = wi ? atomicAdd(counter, wi) : 0u;
+  }
+  __syncthreads();
+  const uint32_t r = s_base1 + s_warp1[wid] + incl - c;
+  __syncthreads();
+  return r;
+}
+
 // ------------------------------------------------------------------ errors
 enum DevErr : uint32_t {
   DE_BARRIER_TIMEOUT = 1u,   // a grid barrier gave up waiting

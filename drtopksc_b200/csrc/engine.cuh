@@ -200,6 +200,54 @@ DRTOPK_DEV void for_each_src(const Src& s, bool from_pairs, uint64_t count, F&& 
   }
 }
 
+// --------------------------------------------------------------- split
+constexpr int SPLIT_E = 8;  // entries per thread per tile
+
+// One level's split of a set: keys above N's range -> top list, keys inside
+// -> next set (+ histogram of the next level).  Tiles of blockDim*SPLIT_E
+// entries, coalesced loads, one block-aggregated append per tile.
+template <int KM>
+DRTOPK_DEV void split_tiles(const EngineCfg& c, const Src& s, bool pairs, uint64_t count, const Level& N,
+                            bool want_hist, uint2* top, uint32_t* top_count, uint2* nxt, uint32_t* nxt_count,
+                            uint32_t* s_hist) {
+  const uint64_t T = (uint64_t)blockDim.x * SPLIT_E;
+  for (uint64_t tb = (uint64_t)blockIdx.x * T; tb < count; tb += (uint64_t)gridDim.x * T) {
+    uint32_t val[SPLIT_E], pay[SPLIT_E], key[SPLIT_E];
+    uint32_t up = 0, in = 0, ca = 0, cb = 0;
+#pragma unroll
+    for (int e = 0; e < SPLIT_E; ++e) {
+      const uint64_t i = tb + (uint64_t)e * blockDim.x + threadIdx.x;
+      val[e] = 0; pay[e] = 0;
+      if (i < count) {
+        if (pairs) {
+          uint2 x = ld_cg_v2(reinterpret_cast<const uint32_t*>(s.pairs + i));
+          val[e] = x.x; pay[e] = x.y;
+        } else {
+          val[e] = src_key1<KM>(s, i);
+          pay[e] = (uint32_t)i;
+        }
+      }
+      key[e] = c.key_from_payload ? ~pay[e] : val[e];
+      const bool valid = i < count;
+      const bool u = valid && key[e] > N.hi;
+      const bool w = valid && key[e] >= N.lo && key[e] <= N.hi;
+      up |= (uint32_t)u << e;
+      in |= (uint32_t)w << e;
+      ca += u;
+      cb += w;
+    }
+    Slots2 sl = block_append2(ca, cb, top_count, nxt_count);
+#pragma unroll
+    for (int e = 0; e < SPLIT_E; ++e) {
+      if ((up >> e) & 1u) top[sl.a++] = make_uint2(val[e], pay[e]);
+      if ((in >> e) & 1u) {
+        nxt[sl.b++] = make_uint2(val[e], pay[e]);
+        if (want_hist) atomicAdd(&s_hist[bin_of(key[e], N.lo, N.w, N.wshift)], 1u);
+      }
+    }
+  }
+}
+
 // --------------------------------------------------------------- one run
 // Runs levels until done.  H[0] of the run must hold the histogram of level
 // 0 over the source (with range L0) and H[1] must be zero when called.
@@ -238,31 +286,14 @@ DRTOPK_DEV int run_levels(const EngineCfg& c, const Src& src0, bool src0_pairs, 
     const bool from_pairs = (j == 0) ? src0_pairs : true;
     Src s = src0;
     uint64_t cnt;
-    bool filter;
     if (j == 0) {
       cnt = src0_pairs ? (uint64_t)ld_cg_u32(src0.count_dev) : src0.count;
-      filter = false;  // level 0 range covers the whole source
     } else {
       s.pairs = rb.cbuf[(j - 1) & 1];
       cnt = ld_cg_u32(rb.set_count + j);
-      filter = false;
     }
-    uint2* nxt = rb.cbuf[j & 1];
-    uint32_t* nxt_cnt = rb.set_count + j + 1;
-    const bool kfp = c.key_from_payload;
-    for_each_src<KM>(s, from_pairs, cnt, [&](uint32_t val, uint32_t pay, bool valid) {
-      const uint32_t key = kfp ? ~pay : val;
-      const bool member = valid && (!filter || (key >= L.lo && key <= L.hi));
-      const bool up = member && key > N.hi;
-      const bool in = member && key >= N.lo && key <= N.hi;
-      uint32_t slot = warp_append(up, rb.top_count);
-      if (up) rb.top[slot] = make_uint2(val, pay);
-      uint32_t slot2 = warp_append(in, nxt_cnt);
-      if (in) {
-        nxt[slot2] = make_uint2(val, pay);
-        if (want_hist) atomicAdd(&s_hist[bin_of(key, N.lo, N.w, N.wshift)], 1u);
-      }
-    });
+    split_tiles<KM>(c, s, from_pairs, cnt, N, want_hist, rb.top, rb.top_count, rb.cbuf[j & 1], rb.set_count + j + 1,
+                    s_hist);
     if (want_hist) flush_hist(s_hist, Hn, c.nb);
     if (!grid_barrier(gb)) { ok = false; break; }
     L = N;
@@ -325,12 +356,13 @@ DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_p
   res.kth = (E == 1) ? ld_cg_v2(reinterpret_cast<const uint32_t*>(eq)).x : Lf.lo;
   const uint32_t R = Lf.R;
   if (E == R) {
-    Src s = {};
-    s.pairs = eq;
-    for_each_src<KM>(s, true, E, [&](uint32_t val, uint32_t pay, bool valid) {
-      uint32_t slot = warp_append(valid, rb.top_count);
-      if (valid) rb.top[slot] = make_uint2(val, pay);
-    });
+    // every tied entry is kept: they go after the G = k0 - R entries above
+    const uint64_t G0 = (uint64_t)ld_cg_u32(rb.top_count);
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t Gs = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = g; i < E; i += Gs) rb.top[G0 + i] = ld_cg_v2(reinterpret_cast<const uint32_t*>(eq + i));
+    if (!grid_barrier(gb)) { res.ok = 0; return res; }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(rb.top_count, (uint32_t)E);
     if (!grid_barrier(gb)) res.ok = 0;
     return res;
   }

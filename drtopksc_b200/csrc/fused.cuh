@@ -50,6 +50,8 @@ struct FusedArgs {
   int has_pos;
   const uint32_t* del_minmax;  // [2] from the sampler (bucket mode)
   RunBufs A, AF, C, CF;
+  uint32_t* sel;          // beta path: selected subrange ids [M]
+  uint32_t* sel_count;
   uint2* cand;
   uint32_t* cand_count;
   uint64_t cand_cap;
@@ -94,73 +96,105 @@ DRTOPK_DEV void load4(const FusedArgs& a, uint64_t base, bool vec, uint32_t (&v)
   }
 }
 
-// default path: keys >= thr of the k kept subranges (uint4 granules, S >= 4)
+// candidates >= thr of a list of kept subranges: the default path's k
+// subranges (ids in the .y of the first select's top list) or the beta
+// path's selected list.  Virtual space = count*S keys in uint4 granules (S>=4;
+// S=2 uses 2-key granules); 4 granules per thread per tile, one
+// block-aggregated append per tile.
+constexpr int GATHER_U = 4;
+
 template <int KM>
-DRTOPK_DEV void gather_default(const FusedArgs& a, uint32_t thr, uint32_t* s_hist, uint32_t& mlo, uint32_t& mhi,
-                               bool& ovf) {
+DRTOPK_DEV void gather_list(const FusedArgs& a, const uint2* ids2, const uint32_t* ids1, uint64_t nsub, uint32_t thr,
+                            uint32_t* s_hist, uint32_t& mlo, uint32_t& mhi, bool& ovf) {
   const uint64_t S = 1ull << a.alpha;
-  const uint64_t units = ((uint64_t)a.k * S) >> 2;
-  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t iters = (units + G - 1) / G;
-  for (uint64_t it = 0; it < iters; ++it) {
-    const uint64_t u = it * G + g;
-    bool valid = u < units;
-    uint64_t base = 0;
-    uint32_t v[4] = {0u, 0u, 0u, 0u};
-    if (valid) {
-      const uint64_t q = u << 2;
-      const uint64_t sel = q >> a.alpha;
-      const uint32_t sub = ld_cg_v2(reinterpret_cast<const uint32_t*>(a.A.top + sel)).y;
-      base = ((uint64_t)sub << a.alpha) + (q & (S - 1));
-      load4<KM>(a, base, a.vec_ok && base + 4 <= a.n, v);
-    }
+  const int gshift = a.alpha >= 2 ? 2 : a.alpha;  // log2 keys per granule
+  const int gk = 1 << gshift;
+  const uint64_t units = (nsub * S) >> gshift;
+  const uint64_t T = (uint64_t)blockDim.x * GATHER_U;
+  for (uint64_t tb = (uint64_t)blockIdx.x * T; tb < units; tb += (uint64_t)gridDim.x * T) {
+    uint32_t v[GATHER_U][4];
+    uint64_t base[GATHER_U];
+    uint32_t take = 0, cnt = 0;
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const bool take = valid && (base + e < a.n) && v[e] >= thr;
-      emit_candidate<KM>(a, take, v[e], (uint32_t)(base + e), s_hist, mlo, mhi, ovf);
+    for (int q = 0; q < GATHER_U; ++q) {
+      const uint64_t u = tb + (uint64_t)q * blockDim.x + threadIdx.x;
+      base[q] = 0;
+      v[q][0] = v[q][1] = v[q][2] = v[q][3] = 0u;
+      if (u < units) {
+        const uint64_t pos = u << gshift;
+        const uint64_t sel = pos >> a.alpha;
+        const uint32_t sub = ids2 ? ld_cg_v2(reinterpret_cast<const uint32_t*>(ids2 + sel)).y : ld_cg_u32(ids1 + sel);
+        base[q] = ((uint64_t)sub << a.alpha) + (pos & (S - 1));
+        if (gk == 4) {
+          load4<KM>(a, base[q], a.vec_ok && base[q] + 4 <= a.n, v[q]);
+        } else {
+          for (int e = 0; e < gk; ++e) v[q][e] = (base[q] + e < a.n) ? to_key<KM>(__ldg(a.keys + base[q] + e)) : 0u;
+        }
+        for (int e = 0; e < gk; ++e) {
+          const bool t = (base[q] + e < a.n) && v[q][e] >= thr;
+          take |= (uint32_t)t << (q * 4 + e);
+          cnt += t;
+        }
+      }
     }
+    uint32_t slot = block_append1(cnt, a.cand_count);
+#pragma unroll
+    for (int q = 0; q < GATHER_U; ++q)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if ((take >> (q * 4 + e)) & 1u) {
+          const uint32_t key = v[q][e];
+          if (slot < a.cand_cap) a.cand[slot] = make_uint2(key, (uint32_t)(base[q] + e));
+          else ovf = true;
+          ++slot;
+          if (a.bucket) { mlo = max(mlo, ~key); mhi = max(mhi, key); }
+          else atomicAdd(&s_hist[key >> (32 - a.nbits)], 1u);
+        }
+      }
   }
 }
 
-// beta path: FindTopKRanges_beta fused with the concatenation
+// beta path filter (FindTopKRanges_beta, radixselect.cuh:560-598): per
+// subrange, Max >= thr and Second >= thr -> subrange id to the selected
+// list; Max >= thr only -> Max itself is a candidate (with its position).
+constexpr int FILTER_E = 4;
+
 template <int KM>
-DRTOPK_DEV void filter_gather_beta(const FusedArgs& a, uint32_t thr, uint32_t* s_hist, uint32_t& mlo, uint32_t& mhi,
-                                   bool& ovf, uint32_t& nsel, uint32_t& nlonely) {
-  const uint64_t S = 1ull << a.alpha;
-  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t iters = (a.M + G - 1) / G;
-  for (uint64_t it = 0; it < iters; ++it) {
-    const uint64_t j = it * G + g;
-    bool sel = false, lonely = false;
-    uint32_t m1 = 0;
-    if (j < a.M) {
-      uint2 d = *reinterpret_cast<const uint2*>(a.del + 2 * j);
-      m1 = d.x;
-      sel = d.x >= thr && d.y >= thr;
-      lonely = d.x >= thr && d.y < thr;
-    }
-    nsel += sel;
-    nlonely += lonely;
-    const uint64_t jb = j << a.alpha;
-    uint32_t lidx = (uint32_t)jb;
-    if (lonely && a.has_pos) lidx += a.pos[j];
-    emit_candidate<KM>(a, lonely, m1, lidx, s_hist, mlo, mhi, ovf);
-    if (__any_sync(0xffffffffu, sel)) {
-      for (uint64_t e = 0; e < S; e += 4) {
-        uint32_t v[4] = {0u, 0u, 0u, 0u};
-        if (sel) {
-          if (S >= 4) load4<KM>(a, jb + e, a.vec_ok && jb + e + 4 <= a.n, v);
-          else
-            for (int t = 0; t < (int)S; ++t) v[t] = (jb + t < a.n) ? to_key<KM>(__ldg(a.keys + jb + t)) : 0u;
-        }
+DRTOPK_DEV void filter_beta(const FusedArgs& a, uint32_t thr, uint32_t* s_hist, uint32_t& mlo, uint32_t& mhi,
+                            bool& ovf) {
+  const uint64_t T = (uint64_t)blockDim.x * FILTER_E;
+  for (uint64_t tb = (uint64_t)blockIdx.x * T; tb < a.M; tb += (uint64_t)gridDim.x * T) {
+    uint32_t m1[FILTER_E];
+    uint32_t lon = 0, sel = 0, cl = 0, cs = 0;
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const bool take = sel && (e + t < S) && (jb + e + t < a.n) && v[t] >= thr;
-          emit_candidate<KM>(a, take, v[t], (uint32_t)(jb + e + t), s_hist, mlo, mhi, ovf);
-        }
+    for (int q = 0; q < FILTER_E; ++q) {
+      const uint64_t j = tb + (uint64_t)q * blockDim.x + threadIdx.x;
+      m1[q] = 0;
+      if (j < a.M) {
+        const uint2 d = *reinterpret_cast<const uint2*>(a.del + 2 * j);
+        m1[q] = d.x;
+        const bool s1 = d.x >= thr && d.y >= thr;
+        const bool l1 = d.x >= thr && d.y < thr;
+        sel |= (uint32_t)s1 << q;
+        lon |= (uint32_t)l1 << q;
+        cs += s1;
+        cl += l1;
       }
+    }
+    Slots2 sl = block_append2(cl, cs, a.cand_count, a.sel_count);
+#pragma unroll
+    for (int q = 0; q < FILTER_E; ++q) {
+      const uint64_t j = tb + (uint64_t)q * blockDim.x + threadIdx.x;
+      if ((lon >> q) & 1u) {
+        uint32_t idx = (uint32_t)(j << a.alpha);
+        if (a.has_pos) idx += a.pos[j];
+        if (sl.a < a.cand_cap) a.cand[sl.a] = make_uint2(m1[q], idx);
+        else ovf = true;
+        ++sl.a;
+        if (a.bucket) { mlo = max(mlo, ~m1[q]); mhi = max(mhi, m1[q]); }
+        else atomicAdd(&s_hist[m1[q] >> (32 - a.nbits)], 1u);
+      }
+      if ((sel >> q) & 1u) a.sel[sl.b++] = (uint32_t)j;
     }
   }
 }
@@ -372,10 +406,20 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
       if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
       return;
     }
-    gather_default<KM>(a, thr1, s_hist, mlo, mhi, ovf);
-    nsel = a.k;
+    gather_list<KM>(a, a.A.top, nullptr, a.k, thr1, s_hist, mlo, mhi, ovf);
   } else if (a.path == PATH_BETA) {
-    filter_gather_beta<KM>(a, thr1, s_hist, mlo, mhi, ovf, nsel, nlonely);
+    filter_beta<KM>(a, thr1, s_hist, mlo, mhi, ovf);
+    if (!grid_barrier(gb)) return;
+    const uint32_t nsel_sub = ld_cg_u32(a.sel_count);
+    if (lead) {
+      a.stats[ST_NSEL] = nsel_sub;
+      a.stats[ST_NLONELY] = ld_cg_u32(a.cand_count);
+    }
+    if (nsel_sub > a.M) {
+      if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
+      return;
+    }
+    gather_list<KM>(a, nullptr, a.sel, nsel_sub, thr1, s_hist, mlo, mhi, ovf);
   }
   if (ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
   if (a.path != PATH_PLAIN) {
@@ -388,15 +432,6 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
       if ((threadIdx.x & 31) == 0) { atomicMax(&a.cand_minmax[0], mlo); atomicMax(&a.cand_minmax[1], mhi); }
     } else {
       flush_hist(s_hist, a.C.H[0], a.nb);
-    }
-    // selection statistics (n_selected summed over threads)
-    for (int off = 16; off > 0; off >>= 1) {
-      nsel += __shfl_xor_sync(0xffffffffu, nsel, off);
-      nlonely += __shfl_xor_sync(0xffffffffu, nlonely, off);
-    }
-    if ((threadIdx.x & 31) == 0 && a.path == PATH_BETA) {
-      atomicAdd(&a.stats[ST_NSEL], nsel);
-      atomicAdd(&a.stats[ST_NLONELY], nlonely);
     }
   } else {
     // plain select: level-0 statistics straight off the input

@@ -17,6 +17,7 @@ enum CtrlWord : int {
   CW_DEL_MINMAX = 4,   // 2 words
   CW_CAND_MINMAX = 6,  // 2 words
   CW_CAND_COUNT = 8,
+  CW_SEL_COUNT = 9,
   CW_STATS = 16,       // 32 words
   CTRL_HDR_WORDS = 48
 };
@@ -36,6 +37,7 @@ struct Plan {
   size_t fused_smem;
   size_t run_words;
   size_t off_ctrl, ctrl_bytes;
+  size_t off_sel;
   size_t off_del, off_pos, off_Atop, off_Acbuf0, off_Acbuf1;
   size_t off_cand, off_Ccbuf0, off_Ctop;
   size_t off_sort0, off_sort1, off_sortcnt;

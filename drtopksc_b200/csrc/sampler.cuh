@@ -151,12 +151,28 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
     const int R = alpha >= 7 ? (1 << (alpha - 7)) : 1;
     const int dpc = 512 >> alpha;  // delegates per chunk
     uint32_t* stage = s_stage[wib];
-    for (uint64_t ch = gwarp; ch < nchunks; ch += nwarps) {
-      const uint64_t cb = ch << 9;
-      const bool full = a.vec_ok && (cb + 512 <= a.n);
+    // register double buffer: chunk ch+nwarps is in flight while ch is reduced
+    uint32_t kn[4][4];
+    uint64_t ch = gwarp;
+    if (ch < nchunks) {
+      const uint64_t cb0 = ch << 9;
+      const bool full0 = a.vec_ok && (cb0 + 512 <= a.n);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) load_row4<KM>(a, cb0 + r * 128 + lane * 4, pol, full0, kn[r]);
+    }
+    for (; ch < nchunks; ch += nwarps) {
       uint32_t k[4][4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) load_row4<KM>(a, cb + r * 128 + lane * 4, pol, full, k[r]);
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) k[r][q] = kn[r][q];
+      const uint64_t chn = ch + nwarps;
+      if (chn < nchunks) {
+        const uint64_t cbn = chn << 9;
+        const bool fulln = a.vec_ok && (cbn + 512 <= a.n);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) load_row4<KM>(a, cbn + r * 128 + lane * 4, pol, fulln, kn[r]);
+      }
       if (alpha == 1) {
         // two 2-key subranges per lane per row
 #pragma unroll
