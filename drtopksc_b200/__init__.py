@@ -363,3 +363,59 @@ class SegmentResult:
     kth: object
     values: object
     indices: object
+
+
+class Batch:
+    """Batched top-k: many segments of one key buffer in one persistent launch
+    (drtopk_batch_*).  Keys of all segments live in one 32-bit buffer (float
+    segments as their bit patterns); outputs are packed per segment."""
+
+    def __init__(self, device: int = 0):
+        self._b = ctypes.c_void_p()
+        self.device = device
+        check(lib().drtopk_batch_create(ctypes.byref(self._b), device), "drtopk_batch_create")
+        self.nseg = 0
+        self.out_offsets = None
+
+    def close(self):
+        if self._b:
+            lib().drtopk_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def plan(self, offsets, ks, dtypes=None, sorted: bool = False):
+        import numpy as np
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        kk = np.ascontiguousarray(ks, dtype=np.uint32)
+        nseg = kk.size
+        dt = np.ascontiguousarray(dtypes if dtypes is not None else np.zeros(nseg), dtype=np.int32)
+        check(lib().drtopk_batch_plan(self._b, nseg, off.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                      kk.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                      dt.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(bool(sorted))),
+              "drtopk_batch_plan")
+        self.nseg = nseg
+        self.out_offsets = np.concatenate([[0], np.cumsum(kk.astype(np.int64))])
+        return self
+
+    def run(self, keys, kth, vals=None, idx=None, graph: bool = False, stream=None):
+        fn = lib().drtopk_batch_run_graph if graph else lib().drtopk_batch_run
+        check(fn(self._b, keys.data_ptr(), kth.data_ptr(), vals.data_ptr() if vals is not None else None,
+                 idx.data_ptr() if idx is not None else None, _stream_ptr(stream)), "drtopk_batch_run")
+
+    def sync_check(self, stream=None):
+        check(lib().drtopk_batch_sync_check(self._b, _stream_ptr(stream)), "drtopk_batch_sync_check")
+
+    def describe(self):
+        import numpy as np
+        a = np.zeros(self.nseg, dtype=np.int32)
+        al = np.zeros(self.nseg, dtype=np.int32)
+        be = np.zeros(self.nseg, dtype=np.int32)
+        P = ctypes.POINTER(ctypes.c_int)
+        check(lib().drtopk_batch_describe(self._b, a.ctypes.data_as(P), al.ctypes.data_as(P), be.ctypes.data_as(P)),
+              "drtopk_batch_describe")
+        return a, al, be

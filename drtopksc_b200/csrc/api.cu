@@ -226,7 +226,10 @@ void layout(Plan* P, bool want_idx) {
   const uint64_t k = P->k;
   P->has_pos = (P->path == PATH_BETA && want_idx) ? 1 : 0;
   // control block (zeroed each call)
-  P->run_words = 3 * P->nb + (MAX_LEVELS + 2) + 1;
+  // each run's histograms hold max(nb, 256) bins: the tie-fill sub-run
+  // always uses 8-bit digits even when the bucket variant has fewer buckets
+  P->hist_words = std::max(P->nb, 256);
+  P->run_words = 3 * P->hist_words + (MAX_LEVELS + 2) + 1;
   size_t ctrl_words = CTRL_HDR_WORDS + 4 * (size_t)P->run_words + 8 * 256;
   P->off_ctrl = take(ctrl_words * 4);
   P->ctrl_bytes = ctrl_words * 4;
@@ -428,10 +431,10 @@ static RunBufs run_bufs(char* ctrl, const Plan& P, int which) {
   uint32_t* base = reinterpret_cast<uint32_t*>(ctrl) + CTRL_HDR_WORDS + (size_t)which * P.run_words;
   RunBufs r;
   r.H[0] = base;
-  r.H[1] = base + P.nb;
-  r.H[2] = base + 2 * P.nb;
-  r.set_count = base + 3 * P.nb;
-  r.top_count = base + 3 * P.nb + MAX_LEVELS + 2;
+  r.H[1] = base + P.hist_words;
+  r.H[2] = base + 2 * P.hist_words;
+  r.set_count = base + 3 * P.hist_words;
+  r.top_count = base + 3 * P.hist_words + MAX_LEVELS + 2;
   r.cbuf[0] = r.cbuf[1] = nullptr;
   r.top = nullptr;
   return r;

@@ -47,6 +47,16 @@ DRTOPK_DEV uint4 ld_stream_v4(const uint32_t* p, uint64_t pol) {
   return r;
 }
 
+// Same read-only path but allocating in L1 (for warp layouts where two
+// instructions split each 32-byte sector).
+DRTOPK_DEV uint4 ld_l1_v4(const uint32_t* p, uint64_t pol) {
+  uint4 r;
+  asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+               : "l"(p), "l"(pol));
+  return r;
+}
+
 DRTOPK_DEV uint32_t ld_stream_u32(const uint32_t* p, uint64_t pol) {
   uint32_t r;
   asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(r) : "l"(p), "l"(pol));

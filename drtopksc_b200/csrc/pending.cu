@@ -2,13 +2,6 @@
 #include "../../include/drtopk.h"
 
 extern "C" {
-drtopk_status_t drtopk_batch_create(drtopk_batch_t* b, int) { if (b) *b = nullptr; return DRTOPK_EUNSUPPORTED; }
-drtopk_status_t drtopk_batch_destroy(drtopk_batch_t) { return DRTOPK_OK; }
-drtopk_status_t drtopk_batch_plan(drtopk_batch_t, int, const uint64_t*, const uint32_t*, const int*, int) { return DRTOPK_EUNSUPPORTED; }
-drtopk_status_t drtopk_batch_run(drtopk_batch_t, const void*, void*, void*, int64_t*, void*) { return DRTOPK_EUNSUPPORTED; }
-drtopk_status_t drtopk_batch_run_graph(drtopk_batch_t, const void*, void*, void*, int64_t*, void*) { return DRTOPK_EUNSUPPORTED; }
-drtopk_status_t drtopk_batch_sync_check(drtopk_batch_t, void*) { return DRTOPK_EUNSUPPORTED; }
-drtopk_status_t drtopk_batch_describe(drtopk_batch_t, int*, int*, int*) { return DRTOPK_EUNSUPPORTED; }
 drtopk_status_t drtopk_server_create(drtopk_server_t* s, int, size_t, int) { if (s) *s = nullptr; return DRTOPK_EUNSUPPORTED; }
 drtopk_status_t drtopk_server_destroy(drtopk_server_t) { return DRTOPK_OK; }
 drtopk_status_t drtopk_server_submit(drtopk_server_t, const void*, drtopk_dtype_t, uint64_t, uint64_t, int, void*, int64_t*, uint64_t*) { return DRTOPK_EUNSUPPORTED; }

@@ -36,6 +36,7 @@ struct Plan {
   int fused_grid, sample_grid;
   size_t fused_smem;
   size_t run_words;
+  int hist_words;
   size_t off_ctrl, ctrl_bytes;
   size_t off_sel;
   size_t off_del, off_pos, off_Atop, off_Acbuf0, off_Acbuf1;

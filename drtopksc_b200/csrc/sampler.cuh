@@ -83,6 +83,29 @@ DRTOPK_DEV void load_row4(const SampleArgs& a, uint64_t base, uint64_t pol, bool
   }
 }
 
+// a lane's 16 consecutive keys as 16/2^SA whole subranges of 2^SA keys
+template <int SA, int BETA, bool POS>
+DRTOPK_DEV void small_subranges(const uint32_t (&k)[4][4], uint32_t* stage, uint16_t* pstage, unsigned lane) {
+  constexpr int S_ = 1 << SA, per = 16 >> SA;
+#pragma unroll
+  for (int j = 0; j < per; ++j) {
+    Acc acc = {0u, 0u, 0u};
+#pragma unroll
+    for (int t = 0; t < S_; ++t) {
+      const int q = j * S_ + t;
+      acc_push<BETA, POS>(acc, k[q >> 2][q & 3], (uint32_t)t);
+    }
+    const int d = lane * per + j;
+    if (BETA == 2) {
+      stage[2 * d] = acc.a1;
+      stage[2 * d + 1] = acc.a2;
+      if (POS) pstage[d] = (uint16_t)acc.p1;
+    } else {
+      stage[d] = acc.a1;
+    }
+  }
+}
+
 template <int KM, int BETA, bool POS>
 __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
   __shared__ uint32_t s_hist[256];
@@ -144,82 +167,68 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
       }
     }
   } else {
-    // ---- 512-key chunks holding 512/S subranges; lanes of a subrange:
-    // G = min(32, S/4) lanes per row, R = max(1, S/128) rows per subrange.
+    // ---- 512-key chunks holding 512/S subranges (alpha 1..8).  Lane l owns
+    // 16 keys: with G = max(1, S/16) lanes per subrange, its i-th uint4 is
+    // uint4 (l/G)*4G + (l%G) + G*i of the chunk, so for S >= 16 all 16 keys
+    // belong to one subrange (reduced in-lane, then log2(G) xor steps) and
+    // for S < 16 they are 16/S whole subranges (no shuffles).  Accesses stay
+    // within 128-byte runs of 16*G bytes; the loads allocate in L1 so the
+    // second half of a shared sector hits there.
     const uint64_t nchunks = (a.n + 511) >> 9;
-    const int G = alpha >= 7 ? 32 : (alpha >= 2 ? (1 << (alpha - 2)) : 1);
-    const int R = alpha >= 7 ? (1 << (alpha - 7)) : 1;
+    const int G = alpha >= 4 ? min(32, 1 << (alpha - 4)) : 1;
     const int dpc = 512 >> alpha;  // delegates per chunk
     uint32_t* stage = s_stage[wib];
+    const int grp = lane / G, gl = lane % G;
+    auto uidx = [&](int i) { return grp * 4 * G + gl + G * i; };  // uint4 index inside the chunk
+    auto load_chunk = [&](uint64_t ch, uint32_t (&k)[4][4]) {
+      const uint64_t cb = ch << 9;
+      const bool full = a.vec_ok && (cb + 512 <= a.n);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const uint64_t base = cb + 4 * (uint64_t)uidx(i);
+        if (full) {
+          uint4 v = ld_l1_v4(a.keys + base, pol);
+          k[i][0] = to_key<KM>(v.x); k[i][1] = to_key<KM>(v.y); k[i][2] = to_key<KM>(v.z); k[i][3] = to_key<KM>(v.w);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) k[i][e] = (base + e < a.n) ? to_key<KM>(ld_stream_u32(a.keys + base + e, pol)) : 0u;
+        }
+      }
+    };
     // register double buffer: chunk ch+nwarps is in flight while ch is reduced
     uint32_t kn[4][4];
     uint64_t ch = gwarp;
-    if (ch < nchunks) {
-      const uint64_t cb0 = ch << 9;
-      const bool full0 = a.vec_ok && (cb0 + 512 <= a.n);
-#pragma unroll
-      for (int r = 0; r < 4; ++r) load_row4<KM>(a, cb0 + r * 128 + lane * 4, pol, full0, kn[r]);
-    }
+    if (ch < nchunks) load_chunk(ch, kn);
     for (; ch < nchunks; ch += nwarps) {
       uint32_t k[4][4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) k[r][q] = kn[r][q];
+        for (int e = 0; e < 4; ++e) k[i][e] = kn[i][e];
       const uint64_t chn = ch + nwarps;
-      if (chn < nchunks) {
-        const uint64_t cbn = chn << 9;
-        const bool fulln = a.vec_ok && (cbn + 512 <= a.n);
+      if (chn < nchunks) load_chunk(chn, kn);
+      if (alpha >= 4) {
+        Acc acc = {0u, 0u, 0u};
 #pragma unroll
-        for (int r = 0; r < 4; ++r) load_row4<KM>(a, cbn + r * 128 + lane * 4, pol, fulln, kn[r]);
-      }
-      if (alpha == 1) {
-        // two 2-key subranges per lane per row
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int d = r * 64 + lane * 2 + h;
-            uint32_t x0 = k[r][2 * h], x1 = k[r][2 * h + 1];
-            if (BETA == 2) {
-              stage[2 * d] = max(x0, x1);
-              stage[2 * d + 1] = min(x0, x1);
-              if (POS) s_pstage[wib][d] = (x1 > x0) ? 1 : 0;
-            } else {
-              stage[d] = max(x0, x1);
-            }
+          for (int e = 0; e < 4; ++e) acc_push<BETA, POS>(acc, k[i][e], (uint32_t)(4 * (gl + G * i) + e));
+        for (int off = 1; off < G; off <<= 1) acc_merge<BETA, POS>(acc, acc_shfl_xor<BETA, POS>(acc, off));
+        if (gl == 0) {
+          if (BETA == 2) {
+            stage[2 * grp] = acc.a1;
+            stage[2 * grp + 1] = acc.a2;
+            if (POS) s_pstage[wib][grp] = (uint16_t)acc.p1;
+          } else {
+            stage[grp] = acc.a1;
           }
+        }
+      } else if (alpha == 3) {
+        small_subranges<3, BETA, POS>(k, stage, s_pstage[wib], lane);
+      } else if (alpha == 2) {
+        small_subranges<2, BETA, POS>(k, stage, s_pstage[wib], lane);
       } else {
-        Acc row[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          row[r] = {0u, 0u, 0u};
-#pragma unroll
-          for (int q = 0; q < 4; ++q) acc_push<BETA, POS>(row[r], k[r][q], (uint32_t)(r * 128 + lane * 4 + q));
-        }
-        // combine rows of the same subrange (S = 256: rows {0,1},{2,3})
-        if (R == 2) {
-          acc_merge<BETA, POS>(row[0], row[1]);
-          acc_merge<BETA, POS>(row[2], row[3]);
-          row[1] = row[2];
-        }
-        const int ngroups = 4 / R;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          if (r < ngroups) {
-            for (int off = 1; off < G; off <<= 1) acc_merge<BETA, POS>(row[r], acc_shfl_xor<BETA, POS>(row[r], off));
-            if ((lane & (G - 1)) == 0) {
-              const int d = r * (32 / G) + lane / G;
-              if (BETA == 2) {
-                stage[2 * d] = row[r].a1;
-                stage[2 * d + 1] = row[r].a2;
-                if (POS) s_pstage[wib][d] = (uint16_t)(row[r].p1 & (S - 1));
-              } else {
-                stage[d] = row[r].a1;
-              }
-            }
-          }
-        }
+        small_subranges<1, BETA, POS>(k, stage, s_pstage[wib], lane);
       }
       __syncwarp();
       // coalesced copy-out of this chunk's delegates (skip subranges >= M)

@@ -1,0 +1,313 @@
+// segmented.cuh -- batched Dr.Top-k: many independent top-k problems of
+// uneven length and k in ONE persistent launch driven by a ticket queue.
+//
+// Tasks, in ticket order:
+//   [sampler tasks]  one per CH-key chunk of every delegate segment: the
+//                    chunk's subrange maxima (sampleMax, reference
+//                    radixselect.cuh:882-918) into the segment's delegate
+//                    slice; the task then bumps the segment's done counter.
+//   [select tasks]   one per segment, one CTA each: waits (bounded) for the
+//                    segment's sampler tasks, then runs the whole Dr.Top-k
+//                    tail inside the CTA --
+//                      first select   exact k-th largest delegate D
+//                                     (block radix select, 8-bit digits)
+//                      keep           subranges with delegate > D, then the
+//                                     lowest-id ones == D up to k
+//                      concatenate    their keys >= D, in index order
+//                      second select  exact k-th key K over the candidates
+//                      top list       keys > K, then the lowest-index == K
+//                    plain segments skip straight to the last two steps on
+//                    the raw keys.
+// A select task only waits on sampler tasks with smaller tickets, which were
+// taken by CTAs already running, so the queue cannot deadlock; the wait is
+// bounded anyway (error flag, segment marked failed).
+// Every scan inside a CTA is in index order, so results are deterministic
+// and ties go to the lowest index without any sort.
+#pragma once
+
+#include "common.cuh"
+
+namespace drtopk {
+
+constexpr int SEG_THREADS = 256;
+constexpr int SEG_CH = 32768;        // keys per sampler task
+constexpr int SEG_MAX_K = 4096;      // per-segment k limit of the batched form
+
+enum SegMode : int { SEG_PLAIN = 0, SEG_DELEGATE = 1 };
+
+struct SegDesc {
+  uint64_t key_off;   // first key of the segment in the batch key array
+  uint64_t del_off;   // delegate slice
+  uint64_t cand_off;  // candidate slice (capacity k * 2^alpha)
+  uint64_t out_off;   // first output slot
+  uint32_t len, k;
+  int32_t km, mode, alpha, ntasks;
+};
+
+struct SegArgs {
+  const uint32_t* keys;
+  const SegDesc* seg;
+  const uint2* tasks;     // sampler tasks: (segment, chunk)
+  uint32_t n_sampler_tasks;
+  uint32_t nseg;
+  uint32_t* del_pool;
+  uint2* cand_pool;
+  uint32_t* done;         // per segment: sampler tasks finished
+  uint32_t* ticket;
+  uint32_t* err;
+  uint32_t* seg_err;      // per segment: nonzero = failed
+  uint32_t* out_kth;
+  uint32_t* out_vals;
+  int64_t* out_idx;
+  int sorted;
+};
+
+DRTOPK_DEV uint32_t to_key_rt(uint32_t u, int km) {
+  if (km == KM_F32 || km == KM_F32_MIN) u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+  if (km == KM_U32_MIN || km == KM_F32_MIN) u = ~u;
+  return u;
+}
+
+// ------------------------------------------------------------ sampler task
+DRTOPK_DEV void seg_sample_chunk(const SegArgs& a, const SegDesc& d, uint32_t chunk) {
+  const uint32_t* keys = a.keys + d.key_off;
+  const uint64_t len = d.len;
+  const int alpha = d.alpha;
+  const uint64_t S = 1ull << alpha;
+  const uint64_t c0 = (uint64_t)chunk * SEG_CH, c1 = min(len, c0 + SEG_CH);
+  uint32_t* del = a.del_pool + d.del_off;
+  const bool vec = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0;
+  const unsigned lane = threadIdx.x & 31u;
+  const int wid = threadIdx.x >> 5, nw = SEG_THREADS / 32;
+  // one warp per subrange (chunks are multiples of S)
+  for (uint64_t j = (c0 >> alpha) + wid; j < ((c1 + S - 1) >> alpha); j += nw) {
+    const uint64_t b = j << alpha, e = min(len, b + S);
+    uint32_t m = 0;
+    for (uint64_t p = b + lane * 4; p < e; p += 128) {
+      if (vec && p + 4 <= e) {
+        uint4 v = __ldg(reinterpret_cast<const uint4*>(keys + p));
+        m = max(max(m, max(to_key_rt(v.x, d.km), to_key_rt(v.y, d.km))),
+                max(to_key_rt(v.z, d.km), to_key_rt(v.w, d.km)));
+      } else {
+        for (int q = 0; q < 4; ++q)
+          if (p + q < e) m = max(m, to_key_rt(__ldg(keys + p + q), d.km));
+      }
+    }
+    m = __reduce_max_sync(0xffffffffu, m);
+    if (lane == 0) del[j] = m;
+  }
+}
+
+// ------------------------------------------------------------ block select
+// Exact k-th largest key over a set given by get(i) -> key for i < n (keys
+// that the caller maps), 8-bit digits, 4 passes; returns K and, through
+// n_above, how many keys are > K.  All threads.
+template <typename G>
+DRTOPK_DEV uint32_t block_kth(uint64_t n, uint32_t k, G&& get, uint32_t* s_hist, uint32_t& n_above) {
+  __shared__ uint32_t s_bin, s_above;
+  uint32_t lo = 0, R = k;
+  for (int d = 3; d >= 0; --d) {
+    const int sh = 8 * d;
+    const uint32_t mask_hi = (d == 3) ? 0u : (0xffffffffu << (sh + 8));
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) s_hist[i] = 0;
+    __syncthreads();
+    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t v = get(i);
+      if ((v & mask_hi) == lo) atomicAdd(&s_hist[(v >> sh) & 255u], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      // warp 0: suffix scan of 256 bins (8 per lane, from the top)
+      const unsigned lane = threadIdx.x;
+      uint32_t c[8], loc = 0;
+      for (int q = 0; q < 8; ++q) { c[q] = s_hist[255 - (lane * 8 + q)]; loc += c[q]; }
+      uint32_t incl = loc;
+      for (int off = 1; off < 32; off <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+        if ((int)lane >= off) incl += y;
+      }
+      const uint32_t before = incl - loc;  // keys in bins above this lane's bins
+      if (before < R && R <= incl) {
+        uint32_t acc = before;
+        for (int q = 0; q < 8; ++q) {
+          if (acc + c[q] >= R) { s_bin = 255 - (lane * 8 + q); s_above = acc; break; }
+          acc += c[q];
+        }
+      }
+    }
+    __syncthreads();
+    lo |= s_bin << sh;
+    R -= s_above;
+    __syncthreads();
+  }
+  n_above = k - R;
+  return lo;
+}
+
+// Ordered selection: walks i = 0..n-1 in order and keeps every i with
+// key > K, plus the first `need_eq` with key == K; emit(slot, i) receives
+// consecutive slots in index order.  Returns the number kept.
+template <typename G, typename E>
+DRTOPK_DEV uint32_t block_ordered_take(uint64_t n, uint32_t K, uint32_t need_eq, G&& get, E&& emit) {
+  __shared__ uint32_t s_w[2][SEG_THREADS / 32];
+  __shared__ uint32_t s_run[2];
+  if (threadIdx.x == 0) { s_run[0] = 0; s_run[1] = 0; }
+  __syncthreads();
+  const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  for (uint64_t base = 0; base < n; base += blockDim.x) {
+    const uint64_t i = base + threadIdx.x;
+    uint32_t v = 0;
+    const bool valid = i < n;
+    if (valid) v = get(i);
+    const bool gt = valid && v > K, eq = valid && v == K;
+    const unsigned bg = __ballot_sync(0xffffffffu, gt), be = __ballot_sync(0xffffffffu, eq);
+    if (lane == 0) { s_w[0][wid] = __popc(bg); s_w[1][wid] = __popc(be); }
+    __syncthreads();
+    uint32_t pg = 0, pe = 0, tg = 0, te = 0;
+    for (int w = 0; w < SEG_THREADS / 32; ++w) {
+      if (w < (int)wid) { pg += s_w[0][w]; pe += s_w[1][w]; }
+      tg += s_w[0][w];
+      te += s_w[1][w];
+    }
+    const uint32_t lm = (1u << lane) - 1u;
+    const uint32_t rg = s_run[0] + pg + __popc(bg & lm);   // rank among > K so far
+    const uint32_t re = s_run[1] + pe + __popc(be & lm);   // rank among == K so far
+    const bool take_eq = eq && re < need_eq;
+    // slots: all > K and the taken == K, interleaved in index order
+    const uint32_t eq_before = min(re, need_eq);
+    if (gt) emit(rg + eq_before, i);
+    if (take_eq) emit(rg + re, i);
+    __syncthreads();
+    if (threadIdx.x == 0) { s_run[0] += tg; s_run[1] += te; }
+    __syncthreads();
+  }
+  const uint32_t kept = s_run[0] + min(s_run[1], need_eq);
+  __syncthreads();
+  return kept;
+}
+
+// ------------------------------------------------------------ kernel
+__global__ void __launch_bounds__(SEG_THREADS) k_segmented(SegArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  uint32_t* s_hist = s_dyn;                                              // 256
+  uint2* s_top = reinterpret_cast<uint2*>(s_dyn + 256);                  // SEG_MAX_K
+  uint32_t* s_sel = s_dyn + 256 + 2 * SEG_MAX_K;                         // SEG_MAX_K
+  __shared__ uint32_t s_ticket;
+  __shared__ uint32_t s_cnt;
+  const uint32_t total = a.n_sampler_tasks + a.nseg;
+  for (;;) {
+    if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1u);
+    __syncthreads();
+    const uint32_t t = s_ticket;
+    __syncthreads();
+    if (t >= total) break;
+    if (t < a.n_sampler_tasks) {
+      const uint2 task = a.tasks[t];
+      const SegDesc d = a.seg[task.x];
+      seg_sample_chunk(a, d, task.y);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(a.done + task.x, 1u);
+      }
+      continue;
+    }
+    const uint32_t s = t - a.n_sampler_tasks;
+    const SegDesc d = a.seg[s];
+    const uint32_t* keys = a.keys + d.key_off;
+    const uint32_t k = d.k;
+    if (d.mode == SEG_DELEGATE) {
+      // wait for this segment's sampler tasks (bounded)
+      if (threadIdx.x == 0) {
+        uint32_t it = 0, ok = 1;
+        while (ld_acquire_gpu(a.done + s) < (uint32_t)d.ntasks) {
+          if (++it > (1u << 24)) { ok = 0; break; }
+          __nanosleep(128);
+        }
+        if (!ok) { atomicOr(a.err, (uint32_t)DE_BARRIER_TIMEOUT); a.seg_err[s] = 1; }
+        s_cnt = ok;
+      }
+      __syncthreads();
+      if (!s_cnt) continue;
+      const uint32_t* del = a.del_pool + d.del_off;
+      const uint64_t S = 1ull << d.alpha;
+      const uint64_t M = ((uint64_t)d.len + S - 1) >> d.alpha;
+      auto getd = [&](uint64_t i) { return ld_cg_u32(del + i); };
+      uint32_t gtD = 0;
+      const uint32_t D = block_kth(M, k, getd, s_hist, gtD);
+      // keep: delegates > D, then the lowest ids == D, up to k (ascending ids)
+      block_ordered_take(M, D, k - gtD, getd, [&](uint32_t slot, uint64_t i) { s_sel[slot] = (uint32_t)i; });
+      __syncthreads();
+      // concatenate keys >= D of the kept subranges, in index order; only the
+      // last kept subrange can be the segment's partial tail, so the virtual
+      // span is clipped there
+      uint2* cand = a.cand_pool + d.cand_off;
+      uint64_t vspan = (uint64_t)k << d.alpha;
+      if (s_sel[k - 1] == M - 1) vspan -= (M << d.alpha) - d.len;
+      auto getv = [&](uint64_t q) -> uint32_t {
+        const uint64_t pos = ((uint64_t)s_sel[q >> d.alpha] << d.alpha) + (q & (S - 1));
+        return to_key_rt(__ldg(keys + pos), d.km);
+      };
+      auto putv = [&](uint32_t slot, uint64_t q) {
+        const uint64_t pos = ((uint64_t)s_sel[q >> d.alpha] << d.alpha) + (q & (S - 1));
+        cand[slot] = make_uint2(getv(q), (uint32_t)pos);
+      };
+      // keys >= D: "> D-1", or everything when D == 0
+      const uint32_t nc = (D == 0) ? block_ordered_take(vspan, 0u, 0xffffffffu, getv, putv)
+                                   : block_ordered_take(vspan, D - 1, 0u, getv, putv);
+      __syncthreads();
+      auto getc = [&](uint64_t i) { return ld_cg_v2(reinterpret_cast<const uint32_t*>(cand + i)).x; };
+      uint32_t gtK = 0;
+      const uint32_t K = block_kth(nc, k, getc, s_hist, gtK);
+      block_ordered_take(nc, K, k - gtK, getc, [&](uint32_t slot, uint64_t i) {
+        s_top[slot] = ld_cg_v2(reinterpret_cast<const uint32_t*>(cand + i));
+      });
+      if (threadIdx.x == 0) a.out_kth[s] = from_key(K, d.km);
+    } else {
+      auto getk = [&](uint64_t i) { return to_key_rt(__ldg(keys + i), d.km); };
+      uint32_t gtK = 0;
+      const uint32_t K = block_kth(d.len, k, getk, s_hist, gtK);
+      block_ordered_take(d.len, K, k - gtK, getk,
+                         [&](uint32_t slot, uint64_t i) { s_top[slot] = make_uint2(getk(i), (uint32_t)i); });
+      if (threadIdx.x == 0) a.out_kth[s] = from_key(K, d.km);
+    }
+    __syncthreads();
+    // output (s_top holds the top-k in index order)
+    if (a.sorted) {
+      // bitonic sort of composites (key << 32 | ~idx), descending, in place
+      uint64_t* c64 = reinterpret_cast<uint64_t*>(s_top);
+      int np2 = 1;
+      while (np2 < (int)k) np2 <<= 1;
+      for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+        uint64_t v = 0;
+        if (i < (int)k) { uint2 e = s_top[i]; v = ((uint64_t)e.x << 32) | (uint64_t)(~e.y); }
+        c64[i] = v;
+      }
+      for (int size = 2; size <= np2; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          __syncthreads();
+          for (int i = threadIdx.x; i < np2 / 2; i += blockDim.x) {
+            const int lo = 2 * stride * (i / stride) + (i % stride), hi = lo + stride;
+            const bool desc = ((lo & size) == 0);
+            const uint64_t x = c64[lo], y = c64[hi];
+            if ((x < y) == desc) { c64[lo] = y; c64[hi] = x; }
+          }
+        }
+      __syncthreads();
+      for (int i = threadIdx.x; i < (int)k; i += blockDim.x) {
+        const uint64_t v = c64[i];
+        if (a.out_vals) a.out_vals[d.out_off + i] = from_key((uint32_t)(v >> 32), d.km);
+        if (a.out_idx) a.out_idx[d.out_off + i] = (int64_t)(uint32_t)~(uint32_t)v;
+      }
+    } else {
+      for (int i = threadIdx.x; i < (int)k; i += blockDim.x) {
+        const uint2 e = s_top[i];
+        if (a.out_vals) a.out_vals[d.out_off + i] = from_key(e.x, d.km);
+        if (a.out_idx) a.out_idx[d.out_off + i] = (int64_t)e.y;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace drtopk

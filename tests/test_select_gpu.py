@@ -329,3 +329,28 @@ def test_bitonic_reference_shape_and_normal():
         D.bitonic_topk(t, x.size, 100, 8)  # k not a power of two (sampleBitonic.cu:198-202)
     with pytest.raises(D.DrTopKError):
         D.bitonic_topk(t, x.size, 4096, 8)  # beyond the shared-memory network
+
+
+@pytest.mark.parametrize("alpha", list(range(1, 17)))
+def test_sampler_delegates_every_alpha(alpha):
+    """Delegates written by the sampler equal sampleMax / the top-2 sampler of
+    the reference (restated by the oracle) for every subrange size."""
+    import torch
+
+    import drtopksc_b200 as D
+    log2n = 18
+    x = O.gen("normal", 1 << log2n, alpha)
+    t = to_dev(x)
+    S = 1 << alpha
+    nsub = x.size // S
+    for dflt in ((True, False) if alpha >= 2 else (False,)):
+        k = 1 if dflt else 2
+        beta = 2
+        Max_d = torch.zeros(nsub * beta, dtype=torch.int32, device="cuda")
+        kth, _ = D.sample_radix_select(t, x.size, k, 256, 8, 3, nsub, S, alpha, Max_d, beta, dflt)
+        dl = Max_d.cpu().numpy().view(np.uint32)
+        if dflt:
+            assert np.array_equal(dl[:nsub], O.sample_max(x, alpha)), alpha
+        else:
+            assert np.array_equal(dl, O.sample_top2(x, alpha)), alpha
+        assert kth == O.topk_exact(x, k, False)[0]
