@@ -98,6 +98,7 @@ def lib() -> ctypes.CDLL:
             "drtopk_last_stats": (st, [vp, P(Stats)]),
             "drtopk_autotune": (st, [u64, u64, i32, P(Params)]),
             "drtopk_profile_begin": (st, [vp, i32]),
+            "drtopk_selftest_wait_timeout": (st, [i32, P(ctypes.c_double)]),
             "drtopk_profile_end": (st, [vp, P(ctypes.c_double), P(ctypes.c_double), P(ctypes.c_int)]),
             "drtopk_radix_select": (st, [vp, i32, i32, i32, P(ctypes.c_uint32), i32, i32]),
             "drtopk_bitonic_topk": (st, [vp, i32, i32, i32, i32, vp, vp, P(ctypes.c_uint32)]),

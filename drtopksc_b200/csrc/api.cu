@@ -985,3 +985,53 @@ extern "C" drtopk_status_t drtopk_bitonic_topk(const uint32_t* A_d, int N, int k
   cudaFree(d_kth);
   return s;
 }
+
+// ------------------------------------------------------------ failure-detection self-test
+namespace drtopk {
+__global__ void k_wait_probe(GridBar gb) { grid_barrier(gb); }
+}  // namespace drtopk
+
+extern "C" drtopk_status_t drtopk_selftest_wait_timeout(int device, double* ms_waited) {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cudaSetDevice(device) != cudaSuccess) return DRTOPK_EINVAL;
+  drtopk_status_t s = DRTOPK_OK;
+  uint32_t* w = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaMalloc(&w, 16) != cudaSuccess) s = DRTOPK_ENOMEM;
+  if (s == DRTOPK_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) s = DRTOPK_ECUDA;
+  if (s == DRTOPK_OK && cudaMemset(w, 0, 16) != cudaSuccess) s = DRTOPK_ECUDA;
+  if (s == DRTOPK_OK) {
+    GridBar gb;
+    gb.count = w;
+    gb.gen = w + 1;
+    gb.err = w + 2;
+    gb.nblocks = 2;           // one CTA more than launched: nothing completes the barrier
+    gb.spin_limit = 1u << 22; // ~0.5 s of polls
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(32);
+    cfg.stream = nullptr;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void* args[] = {&gb};
+    cudaEventRecord(e0, nullptr);
+    if (cudaLaunchKernelExC(&cfg, (void*)k_wait_probe, args) != cudaSuccess) s = DRTOPK_ECUDA;
+    cudaEventRecord(e1, nullptr);
+    if (s == DRTOPK_OK && cudaEventSynchronize(e1) != cudaSuccess) s = DRTOPK_ECUDA;
+    uint32_t err = 0;
+    if (s == DRTOPK_OK && cudaMemcpy(&err, w + 2, 4, cudaMemcpyDeviceToHost) != cudaSuccess) s = DRTOPK_ECUDA;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms_waited) *ms_waited = ms;
+    if (s == DRTOPK_OK) s = (err & DE_BARRIER_TIMEOUT) ? DRTOPK_ETIMEOUT : DRTOPK_EDEVICE;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (w) cudaFree(w);
+  cudaSetDevice(cur);
+  return s;
+}

@@ -216,6 +216,7 @@ struct GridBar {
   uint32_t* gen;     // generation number
   uint32_t* err;     // error word (host-visible)
   uint32_t nblocks;
+  uint32_t spin_limit;  // polls before giving up (0: default 2^26)
 };
 
 DRTOPK_DEV bool grid_barrier(const GridBar& gb) {
@@ -234,8 +235,9 @@ DRTOPK_DEV bool grid_barrier(const GridBar& gb) {
         st_release_gpu(gb.gen, g + 1);
       } else {
         uint32_t it = 0;
+        const uint32_t lim = gb.spin_limit ? gb.spin_limit : (1u << 26);
         while (ld_acquire_gpu(gb.gen) == g) {
-          if (++it > (1u << 26)) {
+          if (++it > lim) {
             atomicOr(gb.err, (uint32_t)DE_BARRIER_TIMEOUT);
             ok = 0;
             break;

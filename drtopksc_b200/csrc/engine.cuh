@@ -201,7 +201,7 @@ DRTOPK_DEV void for_each_src(const Src& s, bool from_pairs, uint64_t count, F&& 
 }
 
 // --------------------------------------------------------------- split
-constexpr int SPLIT_E = 8;  // entries per thread per tile
+constexpr int SPLIT_E = 16;  // entries per thread per tile
 
 // One level's split of a set: keys above N's range -> top list, keys inside
 // -> next set (+ histogram of the next level).  Tiles of blockDim*SPLIT_E
@@ -212,7 +212,7 @@ DRTOPK_DEV void split_tiles(const EngineCfg& c, const Src& s, bool pairs, uint64
                             uint32_t* s_hist) {
   const uint64_t T = (uint64_t)blockDim.x * SPLIT_E;
   for (uint64_t tb = (uint64_t)blockIdx.x * T; tb < count; tb += (uint64_t)gridDim.x * T) {
-    uint32_t val[SPLIT_E], pay[SPLIT_E], key[SPLIT_E];
+    uint32_t val[SPLIT_E], pay[SPLIT_E];
     uint32_t up = 0, in = 0, ca = 0, cb = 0;
 #pragma unroll
     for (int e = 0; e < SPLIT_E; ++e) {
@@ -227,10 +227,14 @@ DRTOPK_DEV void split_tiles(const EngineCfg& c, const Src& s, bool pairs, uint64
           pay[e] = (uint32_t)i;
         }
       }
-      key[e] = c.key_from_payload ? ~pay[e] : val[e];
+    }
+#pragma unroll
+    for (int e = 0; e < SPLIT_E; ++e) {
+      const uint64_t i = tb + (uint64_t)e * blockDim.x + threadIdx.x;
+      const uint32_t key = c.key_from_payload ? ~pay[e] : val[e];
       const bool valid = i < count;
-      const bool u = valid && key[e] > N.hi;
-      const bool w = valid && key[e] >= N.lo && key[e] <= N.hi;
+      const bool u = valid && key > N.hi;
+      const bool w = valid && key >= N.lo && key <= N.hi;
       up |= (uint32_t)u << e;
       in |= (uint32_t)w << e;
       ca += u;
@@ -242,7 +246,8 @@ DRTOPK_DEV void split_tiles(const EngineCfg& c, const Src& s, bool pairs, uint64
       if ((up >> e) & 1u) top[sl.a++] = make_uint2(val[e], pay[e]);
       if ((in >> e) & 1u) {
         nxt[sl.b++] = make_uint2(val[e], pay[e]);
-        if (want_hist) atomicAdd(&s_hist[bin_of(key[e], N.lo, N.w, N.wshift)], 1u);
+        const uint32_t key = c.key_from_payload ? ~pay[e] : val[e];
+        if (want_hist) atomicAdd(&s_hist[bin_of(key, N.lo, N.w, N.wshift)], 1u);
       }
     }
   }

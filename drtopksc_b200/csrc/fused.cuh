@@ -101,7 +101,7 @@ DRTOPK_DEV void load4(const FusedArgs& a, uint64_t base, bool vec, uint32_t (&v)
 // path's selected list.  Virtual space = count*S keys in uint4 granules (S>=4;
 // S=2 uses 2-key granules); 4 granules per thread per tile, one
 // block-aggregated append per tile.
-constexpr int GATHER_U = 4;
+constexpr int GATHER_U = 8;
 
 template <int KM>
 DRTOPK_DEV void gather_list(const FusedArgs& a, const uint2* ids2, const uint32_t* ids1, uint64_t nsub, uint32_t thr,
@@ -113,8 +113,9 @@ DRTOPK_DEV void gather_list(const FusedArgs& a, const uint2* ids2, const uint32_
   const uint64_t T = (uint64_t)blockDim.x * GATHER_U;
   for (uint64_t tb = (uint64_t)blockIdx.x * T; tb < units; tb += (uint64_t)gridDim.x * T) {
     uint32_t v[GATHER_U][4];
-    uint64_t base[GATHER_U];
-    uint32_t take = 0, cnt = 0;
+    uint32_t base[GATHER_U];  // key index of the granule (n < 2^32)
+    uint64_t take = 0;
+    uint32_t cnt = 0;
 #pragma unroll
     for (int q = 0; q < GATHER_U; ++q) {
       const uint64_t u = tb + (uint64_t)q * blockDim.x + threadIdx.x;
@@ -124,17 +125,24 @@ DRTOPK_DEV void gather_list(const FusedArgs& a, const uint2* ids2, const uint32_
         const uint64_t pos = u << gshift;
         const uint64_t sel = pos >> a.alpha;
         const uint32_t sub = ids2 ? ld_cg_v2(reinterpret_cast<const uint32_t*>(ids2 + sel)).y : ld_cg_u32(ids1 + sel);
-        base[q] = ((uint64_t)sub << a.alpha) + (pos & (S - 1));
+        base[q] = (uint32_t)(((uint64_t)sub << a.alpha) + (pos & (S - 1)));
         if (gk == 4) {
-          load4<KM>(a, base[q], a.vec_ok && base[q] + 4 <= a.n, v[q]);
+          load4<KM>(a, base[q], a.vec_ok && (uint64_t)base[q] + 4 <= a.n, v[q]);
         } else {
-          for (int e = 0; e < gk; ++e) v[q][e] = (base[q] + e < a.n) ? to_key<KM>(__ldg(a.keys + base[q] + e)) : 0u;
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            v[q][e] = (e < gk && (uint64_t)base[q] + e < a.n) ? to_key<KM>(__ldg(a.keys + base[q] + e)) : 0u;
         }
-        for (int e = 0; e < gk; ++e) {
-          const bool t = (base[q] + e < a.n) && v[q][e] >= thr;
-          take |= (uint32_t)t << (q * 4 + e);
-          cnt += t;
-        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < GATHER_U; ++q) {
+      const uint64_t u = tb + (uint64_t)q * blockDim.x + threadIdx.x;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const bool t = u < units && e < gk && ((uint64_t)base[q] + e < a.n) && v[q][e] >= thr;
+        take |= (uint64_t)t << (q * 4 + e);
+        cnt += t;
       }
     }
     uint32_t slot = block_append1(cnt, a.cand_count);
@@ -142,9 +150,9 @@ DRTOPK_DEV void gather_list(const FusedArgs& a, const uint2* ids2, const uint32_
     for (int q = 0; q < GATHER_U; ++q)
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        if ((take >> (q * 4 + e)) & 1u) {
+        if ((take >> (q * 4 + e)) & 1ull) {
           const uint32_t key = v[q][e];
-          if (slot < a.cand_cap) a.cand[slot] = make_uint2(key, (uint32_t)(base[q] + e));
+          if (slot < a.cand_cap) a.cand[slot] = make_uint2(key, base[q] + e);
           else ovf = true;
           ++slot;
           if (a.bucket) { mlo = max(mlo, ~key); mhi = max(mhi, key); }
@@ -157,7 +165,7 @@ DRTOPK_DEV void gather_list(const FusedArgs& a, const uint2* ids2, const uint32_
 // beta path filter (FindTopKRanges_beta, radixselect.cuh:560-598): per
 // subrange, Max >= thr and Second >= thr -> subrange id to the selected
 // list; Max >= thr only -> Max itself is a candidate (with its position).
-constexpr int FILTER_E = 4;
+constexpr int FILTER_E = 8;
 
 template <int KM>
 DRTOPK_DEV void filter_beta(const FusedArgs& a, uint32_t thr, uint32_t* s_hist, uint32_t& mlo, uint32_t& mhi,

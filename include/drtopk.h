@@ -129,6 +129,14 @@ DRTOPK_API drtopk_status_t drtopk_last_stats(drtopk_handle_t h, drtopk_stats_t* 
 DRTOPK_API drtopk_status_t drtopk_profile_begin(drtopk_handle_t h, int max_calls);
 DRTOPK_API drtopk_status_t drtopk_profile_end(drtopk_handle_t h, double* ms_sample, double* ms_fused, int* ncalls);
 
+/* Failure-detection self-test: launches a one-CTA cooperative kernel whose
+ * grid barrier waits for a second CTA that does not exist.  The bounded wait
+ * gives up (about 0.5 s), records the timeout in the device error word and
+ * the kernel returns, leaving the context usable.  Returns DRTOPK_ETIMEOUT
+ * when the timeout was detected (the expected outcome); *ms_waited receives
+ * the kernel's duration. */
+DRTOPK_API drtopk_status_t drtopk_selftest_wait_timeout(int device, double* ms_waited);
+
 /* Parameters the autotuner picks for (n, k, dtype); p is updated in place. */
 DRTOPK_API drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_t dtype, drtopk_params_t* p);
 
