@@ -121,6 +121,161 @@ def cpu_topk_rate(sample, ks, budget_s: float):
     return done / dt, threads, calls, dt
 
 
+def bench_batched(D, torch, dev, stream, args):
+    """C4: 4096 segments, lengths log-uniform 2^10..2^22, 80% float32 N(0,1)
+    and 20% uint32 uniform, k log-uniform 1..min(len, 1024); one persistent
+    graph-replayed launch vs a loop of plain calls on the same GPU."""
+    import numpy as np
+    rng = np.random.default_rng(2024)
+    nseg = args.batch_segments
+    lens = np.exp2(rng.uniform(10, 22, nseg)).astype(np.int64)
+    f32 = rng.random(nseg) < 0.8
+    ks = np.array([int(np.exp2(rng.uniform(0, np.log2(min(L, 1024))))) for L in lens], dtype=np.uint32)
+    offsets = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+    total = int(offsets[-1])
+    g = torch.Generator(device=dev)
+    g.manual_seed(77)
+    keys = torch.randint(-(1 << 31), 1 << 31, (total,), dtype=torch.int32, device=dev, generator=g)
+    fv = keys.view(torch.float32)
+    for s_ in np.flatnonzero(f32):
+        a, b = int(offsets[s_]), int(offsets[s_ + 1])
+        fv[a:b] = torch.randn(b - a, dtype=torch.float32, device=dev, generator=g)
+    dtypes = f32.astype(np.int32)
+    bt = D.Batch(dev.index or 0).plan(offsets, ks, dtypes, sorted=False)
+    ktot = int(ks.astype(np.int64).sum())
+    kth = torch.zeros(nseg, dtype=torch.int32, device=dev)
+    vals = torch.zeros(ktot, dtype=torch.int32, device=dev)
+    for _ in range(2):
+        bt.run(keys, kth, vals, None, graph=True, stream=stream)
+    bt.sync_check(stream)
+    reps = 5
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        bt.run(keys, kth, vals, None, graph=True, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    bms = e0.elapsed_time(e1) / reps
+    bt.sync_check(stream)
+    # loop of plain calls (autotuned parameters), same outputs
+    h = D.Handle(dev.index or 0)
+    sp = stream.cuda_stream or None
+    kth2 = torch.zeros(nseg, dtype=torch.int32, device=dev)
+    vals2 = torch.zeros(int(ks.max()), dtype=torch.int32, device=dev)
+    plist = [D.autotune(int(lens[i]), int(ks[i]), int(dtypes[i]), D.params(alpha=-2)) for i in range(nseg)]
+
+    def loop():
+        for i in range(nseg):
+            h.select_raw(keys.data_ptr() + 4 * int(offsets[i]), int(dtypes[i]), int(lens[i]), int(ks[i]), plist[i],
+                         kth2.data_ptr() + 4 * i, vals2.data_ptr(), None, sp)
+
+    loop()
+    h.sync_check(stream)
+    e0.record(stream)
+    t0 = time.perf_counter()
+    loop()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    lwall = (time.perf_counter() - t0) * 1e3
+    lms = max(e0.elapsed_time(e1), lwall)
+    exact = bool(torch.equal(kth, kth2))
+    h.close()
+    algo, alpha, _ = bt.describe()
+    bt.close()
+    return {"config": "4096 segments, len log-uniform 2^10..2^22, 80% f32 N(0,1) / 20% u32, k log-uniform "
+                      "1..min(len,1024); one persistent launch (CUDA graph)",
+            "segments": nseg, "total_keys": total, "ms_batch": bms, "req_per_s": nseg / (bms * 1e-3),
+            "keys_per_s": total / (bms * 1e-3), "ms_loop_of_plain_calls": lms,
+            "loop_req_per_s": nseg / (lms * 1e-3), "speedup_vs_loop": lms / bms, "exact_vs_loop": exact,
+            "segments_delegate": int((algo == 0).sum()), "segments_plain": int((algo == 3).sum())}
+
+
+def bench_served(D, torch, dev, stream, args):
+    """C5: Poisson arrivals of requests with N log-uniform 2^12..2^28 keys
+    (u32 uniform, u32 normal or f32 normal, evenly), k log-uniform
+    1..min(N, 2^20); keys resident on the device; 120 GB budget."""
+    import numpy as np
+    rng = np.random.default_rng(31)
+    npool = args.serve_pool
+    g = torch.Generator(device=dev)
+    g.manual_seed(91)
+    pool = []
+    for i in range(npool):
+        n = int(np.exp2(rng.uniform(12, 28)))
+        kind = i % 3
+        if kind == 0:
+            t = torch.randint(-(1 << 31), 1 << 31, (n,), dtype=torch.int32, device=dev, generator=g)
+            dt = D.U32
+        elif kind == 1:
+            z = torch.randn(n, dtype=torch.float64, device=dev, generator=g)
+            t = (z * 2.0 ** 28 + 2.0 ** 31).round().clamp(0, 2 ** 32 - 1).to(torch.int64).to(torch.int32)
+            dt = D.U32
+        else:
+            t = torch.randn(n, dtype=torch.float32, device=dev, generator=g)
+            dt = D.F32
+        pool.append((t, n, dt))
+    R = args.serve_requests
+    reqs = []
+    for r in range(R):
+        t, n, dt = pool[int(rng.integers(npool))]
+        k = int(np.exp2(rng.uniform(0, np.log2(min(n, 1 << 20)))))
+        reqs.append((t, n, dt, k))
+    # loop of plain per-request calls: select + sync + read back k values
+    h = D.Handle(dev.index or 0)
+    kmax = max(r[3] for r in reqs)
+    kth = torch.zeros(1, dtype=torch.int32, device=dev)
+    vals = torch.zeros(kmax, dtype=torch.int32, device=dev)
+    hv = torch.zeros(kmax, dtype=torch.int32, pin_memory=True)
+    ref_kth = []
+
+    def one(t, n, dt, k):
+        p = D.autotune(n, k, dt, D.params(alpha=-2))
+        h.select_raw(t.data_ptr(), dt, n, k, p, kth.data_ptr(), vals.data_ptr(), None, stream.cuda_stream or None)
+        hv[:k].copy_(vals[:k], non_blocking=True)
+        torch.cuda.synchronize(dev)
+        return int(kth.item()) & 0xFFFFFFFF
+
+    for r in reqs[:20]:
+        one(*r)
+    lat_loop = []
+    t0 = time.perf_counter()
+    for r in reqs:
+        a = time.perf_counter()
+        ref_kth.append(one(*r))
+        lat_loop.append((time.perf_counter() - a) * 1e3)
+    loop_s = time.perf_counter() - t0
+    h.close()
+    loop_rps = R / loop_s
+    out = {"config": "Poisson arrivals; N log-uniform 2^12..2^28 (u32 uniform / u32 normal / f32 normal); "
+                     "k log-uniform 1..min(N,2^20); keys resident on the device; 120 GB budget",
+           "requests": R, "pool_arrays": npool, "loop_req_per_s": loop_rps,
+           "loop_p50_ms": float(np.percentile(lat_loop, 50)), "loop_p99_ms": float(np.percentile(lat_loop, 99)),
+           "rates": []}
+    for mult in args.serve_rates:
+        lam = loop_rps * mult
+        srv = D.Server(dev.index or 0, hbm_budget_bytes=120 << 30, max_inflight=64)
+        arr = np.cumsum(rng.exponential(1.0 / lam, R))
+        ids = {}
+        start = time.perf_counter()
+        for i, (t, n, dt, k) in enumerate(reqs):
+            while time.perf_counter() - start < arr[i]:
+                pass
+            ids[srv.submit(t, k, want_indices=False)] = i
+        srv.drain(120000)
+        res = srv.poll(R + 10)
+        srv.close()
+        lat = [r["t_done"] - r["t_submit"] for r in res]
+        span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+        exact = all(r["status"] == 0 for r in res) and all(
+            (int(np.asarray(r["kth"]).view(np.uint32)) == ref_kth[ids[r["id"]]]) for r in res)
+        out["rates"].append({"offered_req_per_s": lam, "req_per_s": len(res) / (span * 1e-3),
+                             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                             "exact_vs_loop": bool(exact)})
+    best = max(out["rates"], key=lambda r: r["req_per_s"])
+    out["speedup_vs_loop"] = best["req_per_s"] / loop_rps
+    return out
+
+
 def run_reference(args):
     """CPU reference arm: rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
@@ -175,6 +330,13 @@ def main():
     ap.add_argument("--alpha-mode", choices=["auto", "ref"], default="auto",
                     help="auto: per-k parameters from the autotuner (headline); ref: the reference's alpha formula")
     ap.add_argument("--no-table", action="store_true", help="skip the per-k tables after the timed region")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-form measurement")
+    ap.add_argument("--batch-segments", type=int, default=4096)
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-pool", type=int, default=48)
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[2.0, 5.0, 20.0],
+                    help="offered load as multiples of the loop's req/s")
     args = ap.parse_args()
 
     if args.impl == "reference":
@@ -281,7 +443,8 @@ def main():
             row = {"ms": round(kms, 4), "keys_per_s": n / (kms * 1e-3),
                    "frac_of_measured_hbm": (4.0 * n + 4.0 * k) / (kms * 1e-3) / (peak * 1e9),
                    "alpha": st["alpha"], "beta": st["beta"], "candidates": st["n_candidates"],
-                   "ms_sample": round(st["ms_sample"], 4)}
+                   "ms_sample": round(st["ms_sample"], 4), "ms_first": round(st["ms_first"], 4),
+                   "ms_concat": round(st["ms_concat"], 4), "ms_second": round(st["ms_second"], 4)}
             if k in REF_V100S_MS and n == 1 << 30:
                 row["reference_v100s_ms"] = REF_V100S_MS[k]
             out[str(k)] = row
@@ -341,6 +504,17 @@ def main():
                "sample": f"first 2^27 keys of the same input, k in {{1,2^10,2^16,2^20}}, {ccalls} calls in "
                          f"{cdt:.1f} s (oracle_topk_mt: per-thread nth_element + merge + sort)"}
 
+    batched = served = None
+    if rank == 0 and world == 1:
+        del keys
+        torch.cuda.empty_cache()
+        if not args.no_batch:
+            batched = bench_batched(D, torch, dev, stream, args)
+            torch.cuda.empty_cache()
+        if not args.no_serve:
+            served = bench_served(D, torch, dev, stream, args)
+            torch.cuda.empty_cache()
+
     if rank == 0:
         out = {
             "metric": "keys/s (exact top-k: k-th value + top-k values, k sweep 2^0..2^24, N=2^30)",
@@ -364,6 +538,8 @@ def main():
             "gpu_launches": 2 * calls,
             "k_sweep": sweep,
             "k_sweep_reference_alpha": sweep_ref,
+            "batched": batched,
+            "served": served,
         }
         print(json.dumps(out), flush=True)
     h.close()

@@ -112,6 +112,7 @@ def lib() -> ctypes.CDLL:
             "drtopk_server_create": (st, [P(vp), i32, sz, i32]),
             "drtopk_server_destroy": (st, [vp]),
             "drtopk_server_submit": (st, [vp, vp, i32, u64, u64, i32, vp, vp, P(ctypes.c_uint64)]),
+            "drtopk_server_submit_device": (st, [vp, vp, i32, u64, u64, i32, vp, vp, P(ctypes.c_uint64)]),
             "drtopk_server_poll": (st, [vp, P(Result), i32, P(ctypes.c_int)]),
             "drtopk_server_cancel": (st, [vp, u64]),
             "drtopk_server_drain": (st, [vp, i32]),
@@ -420,3 +421,83 @@ class Batch:
         check(lib().drtopk_batch_describe(self._b, a.ctypes.data_as(P), al.ctypes.data_as(P), be.ctypes.data_as(P)),
               "drtopk_batch_describe")
         return a, al, be
+
+
+class Server:
+    """Served form (drtopk_server_*): continuous batching of top-k requests
+    under an HBM byte budget.  submit() takes a host numpy array (copied) or
+    a CUDA tensor (kept resident, caller-owned until the request finishes)."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 120 << 30, max_inflight: int = 64):
+        self._s = ctypes.c_void_p()
+        check(lib().drtopk_server_create(ctypes.byref(self._s), device, hbm_budget_bytes, max_inflight),
+              "drtopk_server_create")
+        self._bufs = {}
+
+    def close(self):
+        if self._s:
+            lib().drtopk_server_destroy(self._s)
+            self._s = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def submit(self, keys, k: int, sorted: bool = False, want_values: bool = True, want_indices: bool = True) -> int:
+        """Returns the request id; results (kth, values, indices) come from poll()."""
+        import numpy as np
+        rid = ctypes.c_uint64(0)
+        if hasattr(keys, "is_cuda"):
+            n = keys.numel()
+            dt = _dtype_code(keys)
+            vdtype = np.float32 if dt == F32 else np.uint32
+        else:
+            keys = np.ascontiguousarray(keys)
+            n = keys.size
+            dt = F32 if keys.dtype == np.float32 else U32
+            vdtype = keys.dtype if dt == F32 else np.uint32
+        vals = np.empty(k, dtype=vdtype) if want_values else None
+        idx = np.empty(k, dtype=np.int64) if want_indices else None
+        vp = vals.ctypes.data if vals is not None else None
+        ip = idx.ctypes.data if idx is not None else None
+        if hasattr(keys, "is_cuda"):
+            st = lib().drtopk_server_submit_device(self._s, keys.data_ptr(), dt, n, k, int(bool(sorted)), vp, ip,
+                                                   ctypes.byref(rid))
+        else:
+            st = lib().drtopk_server_submit(self._s, keys.ctypes.data, dt, n, k, int(bool(sorted)), vp, ip,
+                                            ctypes.byref(rid))
+        check(st, "drtopk_server_submit")
+        self._bufs[rid.value] = (keys, vals, idx, dt)
+        return rid.value
+
+    def poll(self, max_results: int = 1024):
+        """List of dicts: id, status, kth, values, indices, t_submit/t_start/t_done (ms)."""
+        import numpy as np
+        arr = (Result * max_results)()
+        cnt = ctypes.c_int(0)
+        st = lib().drtopk_server_poll(self._s, arr, max_results, ctypes.byref(cnt))
+        if st not in (OK, EAGAIN):
+            check(st, "drtopk_server_poll")
+        out = []
+        for i in range(cnt.value):
+            r = arr[i]
+            keys, vals, idx, dt = self._bufs.pop(r.id, (None, None, None, U32))
+            kth = np.array([r.kth], dtype=np.uint32)
+            if dt == F32:
+                kth = kth.view(np.float32)
+            out.append({"id": r.id, "status": r.status, "kth": kth[0], "values": vals, "indices": idx,
+                        "t_submit": r.t_submit_ms, "t_start": r.t_start_ms, "t_done": r.t_done_ms})
+        return out
+
+    def cancel(self, rid: int) -> bool:
+        return lib().drtopk_server_cancel(self._s, rid) == OK
+
+    def drain(self, timeout_ms: int = -1):
+        check(lib().drtopk_server_drain(self._s, timeout_ms), "drtopk_server_drain")
+
+    def usage(self):
+        b, i, q = ctypes.c_size_t(0), ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().drtopk_server_usage(self._s, ctypes.byref(b), ctypes.byref(i), ctypes.byref(q)), "usage")
+        return b.value, i.value, q.value

@@ -11,9 +11,26 @@
 #include <vector>
 
 #include "../../include/drtopk.h"
+#define DRTOPK_DEFINE_SEGMENTED_KERNEL
 #include "segmented.cuh"
 
 using namespace drtopk;
+
+namespace drtopk {
+cudaError_t launch_segmented(const SegArgs& a, int grid, size_t smem, cudaStream_t st) {
+  k_segmented<<<grid, SEG_THREADS, smem, st>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t segmented_shape(int device, int* grid, size_t* smem) {
+  *smem = (size_t)(256 + 3 * SEG_MAX_K) * 4;
+  int occ = 0, sms = 0;
+  cudaError_t e = cudaFuncSetAttribute(k_segmented, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_segmented, SEG_THREADS, *smem);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  *grid = (occ > 0 ? occ : 1) * sms;
+  return e;
+}
+}  // namespace drtopk
 
 struct drtopk_batch {
   int device = 0;
@@ -90,8 +107,7 @@ drtopk_status_t enqueue_batch(drtopk_batch* b, const void* d_keys, void* d_kth, 
   a.out_vals = static_cast<uint32_t*>(d_vals);
   a.out_idx = d_idx;
   a.sorted = b->sorted;
-  k_segmented<<<b->grid, SEG_THREADS, b->smem, st>>>(a);
-  return cudaGetLastError() == cudaSuccess ? DRTOPK_OK : DRTOPK_ECUDA;
+  return launch_segmented(a, b->grid, b->smem, st) == cudaSuccess ? DRTOPK_OK : DRTOPK_ECUDA;
 }
 
 }  // namespace
@@ -189,13 +205,7 @@ extern "C" drtopk_status_t drtopk_batch_plan(drtopk_batch_t b, int nseg, const u
       st = DRTOPK_ECUDA;
   }
   if (st == DRTOPK_OK) {
-    b->smem = (size_t)(256 + 3 * SEG_MAX_K) * 4;
-    int occ = 0, sms = 0;
-    if (cudaFuncSetAttribute(k_segmented, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_segmented, SEG_THREADS, b->smem) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess)
-      st = DRTOPK_ECUDA;
-    b->grid = std::max(1, occ) * sms;
+    if (segmented_shape(b->device, &b->grid, &b->smem) != cudaSuccess) st = DRTOPK_ECUDA;
   }
   if (st == DRTOPK_OK) {
     b->nseg = nseg;

@@ -42,7 +42,18 @@ struct SegDesc {
   uint64_t out_off;   // first output slot
   uint32_t len, k;
   int32_t km, mode, alpha, ntasks;
+  // optional absolute pointers (served form: every request owns its buffers);
+  // when kptr is set the segment's keys are kptr[0..len) and its outputs go
+  // to okth[0], ovals[0..k), oidx[0..k) instead of the packed batch arrays
+  const uint32_t* kptr;
+  uint32_t* okth;
+  uint32_t* ovals;
+  int64_t* oidx;
 };
+
+DRTOPK_DEV const uint32_t* seg_keys(const uint32_t* keys, const SegDesc& d) {
+  return d.kptr ? d.kptr : keys + d.key_off;
+}
 
 struct SegArgs {
   const uint32_t* keys;
@@ -70,7 +81,7 @@ DRTOPK_DEV uint32_t to_key_rt(uint32_t u, int km) {
 
 // ------------------------------------------------------------ sampler task
 DRTOPK_DEV void seg_sample_chunk(const SegArgs& a, const SegDesc& d, uint32_t chunk) {
-  const uint32_t* keys = a.keys + d.key_off;
+  const uint32_t* keys = seg_keys(a.keys, d);
   const uint64_t len = d.len;
   const int alpha = d.alpha;
   const uint64_t S = 1ull << alpha;
@@ -186,6 +197,11 @@ DRTOPK_DEV uint32_t block_ordered_take(uint64_t n, uint32_t K, uint32_t need_eq,
   return kept;
 }
 
+// host helpers (defined with the kernel in batch.cu)
+cudaError_t launch_segmented(const SegArgs& a, int grid, size_t smem, cudaStream_t st);
+cudaError_t segmented_shape(int device, int* grid, size_t* smem);
+
+#ifdef DRTOPK_DEFINE_SEGMENTED_KERNEL
 // ------------------------------------------------------------ kernel
 __global__ void __launch_bounds__(SEG_THREADS) k_segmented(SegArgs a) {
   extern __shared__ __align__(16) uint32_t s_dyn[];
@@ -214,8 +230,11 @@ __global__ void __launch_bounds__(SEG_THREADS) k_segmented(SegArgs a) {
     }
     const uint32_t s = t - a.n_sampler_tasks;
     const SegDesc d = a.seg[s];
-    const uint32_t* keys = a.keys + d.key_off;
+    const uint32_t* keys = seg_keys(a.keys, d);
     const uint32_t k = d.k;
+    uint32_t* o_kth = d.kptr ? d.okth : a.out_kth + s;
+    uint32_t* o_vals = d.kptr ? d.ovals : (a.out_vals ? a.out_vals + d.out_off : nullptr);
+    int64_t* o_idx = d.kptr ? d.oidx : (a.out_idx ? a.out_idx + d.out_off : nullptr);
     if (d.mode == SEG_DELEGATE) {
       // wait for this segment's sampler tasks (bounded)
       if (threadIdx.x == 0) {
@@ -262,14 +281,14 @@ __global__ void __launch_bounds__(SEG_THREADS) k_segmented(SegArgs a) {
       block_ordered_take(nc, K, k - gtK, getc, [&](uint32_t slot, uint64_t i) {
         s_top[slot] = ld_cg_v2(reinterpret_cast<const uint32_t*>(cand + i));
       });
-      if (threadIdx.x == 0) a.out_kth[s] = from_key(K, d.km);
+      if (threadIdx.x == 0 && o_kth) *o_kth = from_key(K, d.km);
     } else {
       auto getk = [&](uint64_t i) { return to_key_rt(__ldg(keys + i), d.km); };
       uint32_t gtK = 0;
       const uint32_t K = block_kth(d.len, k, getk, s_hist, gtK);
       block_ordered_take(d.len, K, k - gtK, getk,
                          [&](uint32_t slot, uint64_t i) { s_top[slot] = make_uint2(getk(i), (uint32_t)i); });
-      if (threadIdx.x == 0) a.out_kth[s] = from_key(K, d.km);
+      if (threadIdx.x == 0 && o_kth) *o_kth = from_key(K, d.km);
     }
     __syncthreads();
     // output (s_top holds the top-k in index order)
@@ -296,18 +315,20 @@ __global__ void __launch_bounds__(SEG_THREADS) k_segmented(SegArgs a) {
       __syncthreads();
       for (int i = threadIdx.x; i < (int)k; i += blockDim.x) {
         const uint64_t v = c64[i];
-        if (a.out_vals) a.out_vals[d.out_off + i] = from_key((uint32_t)(v >> 32), d.km);
-        if (a.out_idx) a.out_idx[d.out_off + i] = (int64_t)(uint32_t)~(uint32_t)v;
+        if (o_vals) o_vals[i] = from_key((uint32_t)(v >> 32), d.km);
+        if (o_idx) o_idx[i] = (int64_t)(uint32_t)~(uint32_t)v;
       }
     } else {
       for (int i = threadIdx.x; i < (int)k; i += blockDim.x) {
         const uint2 e = s_top[i];
-        if (a.out_vals) a.out_vals[d.out_off + i] = from_key(e.x, d.km);
-        if (a.out_idx) a.out_idx[d.out_off + i] = (int64_t)e.y;
+        if (o_vals) o_vals[i] = from_key(e.x, d.km);
+        if (o_idx) o_idx[i] = (int64_t)e.y;
       }
     }
     __syncthreads();
   }
 }
+
+#endif  // DRTOPK_DEFINE_SEGMENTED_KERNEL
 
 }  // namespace drtopk

@@ -1,0 +1,608 @@
+// server.cu -- served form: continuous batching of top-k requests.
+//
+// A worker thread admits queued requests as in-flight slots and the HBM byte
+// budget allow (device memory from a stream-ordered pool, so admission never
+// synchronises the device), and keeps admitting while earlier requests are
+// still on the GPU:
+//   * large requests run one select each, round-robin over a ring of
+//     streams, so their copies and kernels overlap;
+//   * small requests (n <= 2^22, k <= 4096) admitted in the same tick are
+//     grouped into ONE persistent segmented launch (segmented.cuh), each
+//     segment reading and writing its request's own buffers.
+// Results are exact and identical to the plain call (same kernels / same
+// integer arithmetic); completion is detected with events and results are
+// copied into the caller's host buffers before they are reported by poll().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <list>
+#include <map>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "../../include/drtopk.h"
+#include "segmented.cuh"
+
+using namespace drtopk;
+
+namespace {
+
+constexpr int NSTREAMS = 8;
+constexpr uint64_t SMALL_N = 1ull << 22;
+
+struct Req {
+  uint64_t id = 0;
+  drtopk_dtype_t dtype = DRTOPK_U32;
+  uint64_t n = 0, k = 0;
+  int sorted = 0;
+  void* user_vals = nullptr;
+  int64_t* user_idx = nullptr;
+  const void* dkeys_user = nullptr;  // device-resident keys (caller-owned)
+  void* hkeys = nullptr;             // pinned copy of host keys
+  size_t hkeys_cap = 0;
+  char* dmem = nullptr;              // keys copy + outputs (+ workspace for large requests)
+  size_t dbytes = 0;
+  size_t ws_bytes = 0;
+  uint32_t* d_keys = nullptr;
+  uint32_t* d_kth = nullptr;
+  uint32_t* d_vals = nullptr;
+  int64_t* d_idx = nullptr;
+  char* d_ws = nullptr;
+  void* hout = nullptr;              // pinned staging of the outputs
+  size_t hout_cap = 0;
+  void* extra = nullptr;             // pinned batch-descriptor staging released with this request
+  size_t extra_cap = 0;
+  cudaEvent_t ev = nullptr;
+  int stream = 0;
+  double t_submit = 0, t_start = 0, t_done = 0;
+  int status = DRTOPK_OK;
+  bool small = false;
+  char* batch_ws = nullptr;          // shared batch workspace (freed with the last member)
+  std::shared_ptr<int> batch_refs;
+};
+
+struct PinnedCache {
+  std::multimap<size_t, void*> free_;
+  size_t cached = 0;
+  void* get(size_t bytes, size_t* cap) {
+    size_t c = 4096;
+    while (c < bytes) c <<= 1;
+    auto it = free_.lower_bound(c);
+    if (it != free_.end() && it->first <= 2 * c) {
+      void* p = it->second;
+      *cap = it->first;
+      cached -= it->first;
+      free_.erase(it);
+      return p;
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, c, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    *cap = c;
+    return p;
+  }
+  void put(void* p, size_t cap) {
+    if (!p) return;
+    if (cached + cap > (size_t(8) << 30)) {
+      cudaFreeHost(p);
+      return;
+    }
+    free_.emplace(cap, p);
+    cached += cap;
+  }
+  void clear() {
+    for (auto& kv : free_) cudaFreeHost(kv.second);
+    free_.clear();
+    cached = 0;
+  }
+};
+
+inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+struct drtopk_server {
+  int device = 0;
+  size_t budget = 0;
+  int max_inflight = 64;
+  drtopk_handle_t h = nullptr;
+  cudaStream_t streams[NSTREAMS] = {};
+  int next_stream = 0;
+  int seg_grid = 0;
+  size_t seg_smem = 0;
+  std::mutex mu;
+  std::condition_variable cv, done_cv;
+  std::deque<Req*> queue;
+  std::list<Req*> running;
+  std::deque<drtopk_result_t> results;
+  size_t used = 0;
+  int inflight = 0;
+  uint64_t next_id = 1;
+  bool stop = false;
+  std::thread worker;
+  std::chrono::steady_clock::time_point t0;
+  PinnedCache pinned;
+  std::vector<cudaEvent_t> ev_free;
+
+  double now_ms() const {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  cudaEvent_t get_event() {
+    if (!ev_free.empty()) {
+      cudaEvent_t e = ev_free.back();
+      ev_free.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    return e;
+  }
+  // device bytes of a request: keys copy (host mode) + outputs (+ workspace when run alone)
+  drtopk_status_t need_bytes(Req* r, size_t* out) {
+    size_t b = 0;
+    if (!r->dkeys_user) b += al256(r->n * 4);
+    b += al256(4) + al256(r->k * 4) + al256(r->k * 8);
+    if (!r->small) {
+      drtopk_params_t p;
+      drtopk_params_default(&p);
+      p.alpha = -2;
+      p.sorted = r->sorted;
+      size_t ws = 0;
+      drtopk_status_t s = drtopk_workspace_size(r->n, r->k, r->dtype, &p, &ws);
+      if (s != DRTOPK_OK) return s;
+      r->ws_bytes = ws;
+      b += al256(ws);
+    } else {
+      // share of the batch workspace: delegates + candidates of its segment
+      b += al256(r->n / 16 * 4) + al256(r->k * 8 * 256);
+    }
+    *out = b;
+    return DRTOPK_OK;
+  }
+  void complete(Req* r, cudaError_t q);
+  void admit_and_launch();
+  void launch_single(Req* r);
+  void launch_batch(std::vector<Req*>& v);
+  void loop();
+};
+
+void drtopk_server::complete(Req* r, cudaError_t q) {
+  r->t_done = now_ms();
+  if (q != cudaSuccess) r->status = DRTOPK_ECUDA;
+  drtopk_result_t res;
+  std::memset(&res, 0, sizeof(res));
+  res.id = r->id;
+  if (r->status == DRTOPK_OK) {
+    const char* ho = static_cast<const char*>(r->hout);
+    std::memcpy(&res.kth, ho, 4);
+    if (r->user_vals) std::memcpy(r->user_vals, ho + al256(4), r->k * 4);
+    if (r->user_idx) std::memcpy(r->user_idx, ho + al256(4) + al256(r->k * 4), r->k * 8);
+  }
+  res.status = r->status;
+  res.t_submit_ms = r->t_submit;
+  res.t_start_ms = r->t_start;
+  res.t_done_ms = r->t_done;
+  results.push_back(res);
+  used -= r->dbytes;
+  inflight--;
+  pinned.put(r->hkeys, r->hkeys_cap);
+  pinned.put(r->hout, r->hout_cap);
+  pinned.put(r->extra, r->extra_cap);
+  if (r->ev) ev_free.push_back(r->ev);
+  delete r;
+}
+
+void drtopk_server::launch_single(Req* r) {
+  cudaStream_t st = streams[r->stream];
+  drtopk_params_t p;
+  drtopk_params_default(&p);
+  p.alpha = -2;  // autotuned parameters
+  p.sorted = r->sorted;
+  const uint32_t* keys = r->dkeys_user ? static_cast<const uint32_t*>(r->dkeys_user) : r->d_keys;
+  if (!r->dkeys_user && cudaMemcpyAsync(r->d_keys, r->hkeys, r->n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    r->status = DRTOPK_ECUDA;
+  if (r->status == DRTOPK_OK)
+    r->status = drtopk_select_ws(h, keys, r->dtype, r->n, r->k, &p, r->d_kth, r->d_vals, r->d_idx, r->d_ws,
+                                 r->ws_bytes, st);
+  if (r->status == DRTOPK_OK) {
+    char* ho = static_cast<char*>(r->hout);
+    cudaMemcpyAsync(ho, r->d_kth, 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(ho + al256(4), r->d_vals, r->k * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(ho + al256(4) + al256(r->k * 4), r->d_idx, r->k * 8, cudaMemcpyDeviceToHost, st);
+  }
+  cudaFreeAsync(r->dmem, st);
+  r->dmem = nullptr;
+  cudaEventRecord(r->ev, st);
+}
+
+void drtopk_server::launch_batch(std::vector<Req*>& v) {
+  const int si = next_stream;
+  cudaStream_t st = streams[si];
+  next_stream = (next_stream + 1) % NSTREAMS;
+  const int nseg = (int)v.size();
+  std::vector<SegDesc> seg(nseg);
+  std::vector<uint2> tasks;
+  uint64_t del_total = 0, cand_total = 0;
+  for (int s = 0; s < nseg; ++s) {
+    Req* r = v[s];
+    r->stream = si;
+    SegDesc& d = seg[s];
+    std::memset(&d, 0, sizeof(d));
+    d.len = (uint32_t)r->n;
+    d.k = (uint32_t)r->k;
+    d.km = r->dtype == DRTOPK_F32 ? KM_F32 : KM_U32;
+    d.kptr = r->dkeys_user ? static_cast<const uint32_t*>(r->dkeys_user) : r->d_keys;
+    d.okth = r->d_kth;
+    d.ovals = r->d_vals;
+    d.oidx = r->d_idx;
+    // same per-segment choice as the batched form
+    if (d.len <= 32768) {
+      d.mode = SEG_PLAIN;
+    } else {
+      int a = (int)std::lround(std::log2(std::max(2.0, std::sqrt(5.0 * d.len / d.k))));
+      a = std::max(5, std::min(a, 15));
+      while (a > 5 && ((((uint64_t)d.len + (1ull << a) - 1) >> a) < d.k)) a--;
+      if ((((uint64_t)d.len + (1ull << a) - 1) >> a) < d.k) {
+        d.mode = SEG_PLAIN;
+      } else {
+        d.mode = SEG_DELEGATE;
+        d.alpha = a;
+      }
+    }
+    if (d.mode == SEG_DELEGATE) {
+      const uint64_t S = 1ull << d.alpha, M = (d.len + S - 1) >> d.alpha;
+      d.del_off = del_total;
+      del_total += M;
+      d.cand_off = cand_total;
+      cand_total += (uint64_t)d.k * S;
+      d.ntasks = (int)((d.len + SEG_CH - 1) / SEG_CH);
+      for (int c = 0; c < d.ntasks; ++c) tasks.push_back(make_uint2((uint32_t)s, (uint32_t)c));
+    }
+  }
+  size_t off = 0;
+  const size_t o_seg = off;
+  off += al256(sizeof(SegDesc) * nseg);
+  const size_t o_tasks = off;
+  off += al256(sizeof(uint2) * std::max<size_t>(1, tasks.size()));
+  const size_t o_del = off;
+  off += al256(4 * std::max<uint64_t>(1, del_total));
+  const size_t o_cand = off;
+  off += al256(8 * std::max<uint64_t>(1, cand_total));
+  const size_t o_ctrl = off;
+  const size_t ctrl_bytes = 4 * (8 + 2 * (size_t)nseg);
+  off += al256(ctrl_bytes);
+  const size_t hbytes = o_del;  // descriptors + tasks are staged from host
+  char* ws = nullptr;
+  size_t hcap = 0;
+  char* hst = static_cast<char*>(pinned.get(hbytes, &hcap));
+  bool ok = hst && cudaMallocAsync(reinterpret_cast<void**>(&ws), off, st) == cudaSuccess;
+  if (ok) {
+    std::memcpy(hst + o_seg, seg.data(), sizeof(SegDesc) * nseg);
+    if (!tasks.empty()) std::memcpy(hst + o_tasks, tasks.data(), sizeof(uint2) * tasks.size());
+    for (Req* r : v)
+      if (!r->dkeys_user) cudaMemcpyAsync(r->d_keys, r->hkeys, r->n * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(ws, hst, hbytes, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(ws + o_ctrl, 0, ctrl_bytes, st);
+    uint32_t* ctrl = reinterpret_cast<uint32_t*>(ws + o_ctrl);
+    SegArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.keys = nullptr;
+    a.seg = reinterpret_cast<const SegDesc*>(ws + o_seg);
+    a.tasks = reinterpret_cast<const uint2*>(ws + o_tasks);
+    a.n_sampler_tasks = (uint32_t)tasks.size();
+    a.nseg = (uint32_t)nseg;
+    a.del_pool = reinterpret_cast<uint32_t*>(ws + o_del);
+    a.cand_pool = reinterpret_cast<uint2*>(ws + o_cand);
+    a.ticket = ctrl;
+    a.err = ctrl + 1;
+    a.done = ctrl + 8;
+    a.seg_err = ctrl + 8 + nseg;
+    a.sorted = v[0]->sorted;
+    const int grid = std::min<int>(seg_grid, (int)(tasks.size() + nseg));
+    if (launch_segmented(a, std::max(1, grid), seg_smem, st) != cudaSuccess) ok = false;
+    for (Req* r : v) {
+      char* ho = static_cast<char*>(r->hout);
+      cudaMemcpyAsync(ho, r->d_kth, 4, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(ho + al256(4), r->d_vals, r->k * 4, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(ho + al256(4) + al256(r->k * 4), r->d_idx, r->k * 8, cudaMemcpyDeviceToHost, st);
+    }
+    cudaFreeAsync(ws, st);
+  }
+  for (Req* r : v) {
+    if (!ok) r->status = DRTOPK_ENOMEM;
+    cudaFreeAsync(r->dmem, st);
+    r->dmem = nullptr;
+    cudaEventRecord(r->ev, st);
+  }
+  // the descriptor staging buffer may be reused only after the copy ran:
+  // it is released with the last request of the batch (same stream)
+  if (hst) {
+    v.back()->extra = hst;
+    v.back()->extra_cap = hcap;
+  }
+}
+
+void drtopk_server::admit_and_launch() {
+  std::vector<Req*> small;
+  int scanned = 0;
+  const double t = now_ms();
+  for (auto it = queue.begin(); it != queue.end() && inflight < max_inflight && scanned < 256; ++scanned) {
+    Req* r = *it;
+    size_t need = 0;
+    drtopk_status_t s = need_bytes(r, &need);
+    if (s == DRTOPK_OK && budget && need > budget) s = DRTOPK_EBUDGET;
+    if (s != DRTOPK_OK) {
+      it = queue.erase(it);
+      r->status = s;
+      r->t_start = t;
+      inflight++;
+      used += 0;
+      r->dbytes = 0;
+      complete(r, cudaSuccess);
+      continue;
+    }
+    if (budget && used + need > budget) {
+      // head-of-line request too large for now: smaller ones may pass it,
+      // unless it has waited for 50 ms (then it goes first)
+      if (it == queue.begin() && t - r->t_submit > 50.0) break;
+      ++it;
+      continue;
+    }
+    it = queue.erase(it);
+    r->t_start = t;
+    r->dbytes = need;
+    used += need;
+    inflight++;
+    r->ev = get_event();
+    const size_t outb = al256(4) + al256(r->k * 4) + al256(r->k * 8);
+    r->hout = pinned.get(outb, &r->hout_cap);
+    r->stream = next_stream;
+    cudaStream_t st = streams[r->stream];
+    size_t dev = need;
+    if (r->small) dev = (r->dkeys_user ? 0 : al256(r->n * 4)) + outb;  // batch workspace is separate
+    if (!r->hout || cudaMallocAsync(reinterpret_cast<void**>(&r->dmem), dev, st) != cudaSuccess) {
+      cudaGetLastError();
+      r->status = DRTOPK_ENOMEM;
+      cudaEventRecord(r->ev, st);
+      running.push_back(r);
+      continue;
+    }
+    char* p = r->dmem;
+    if (!r->dkeys_user) {
+      r->d_keys = reinterpret_cast<uint32_t*>(p);
+      p += al256(r->n * 4);
+    }
+    r->d_kth = reinterpret_cast<uint32_t*>(p);
+    p += al256(4);
+    r->d_vals = reinterpret_cast<uint32_t*>(p);
+    p += al256(r->k * 4);
+    r->d_idx = reinterpret_cast<int64_t*>(p);
+    p += al256(r->k * 8);
+    r->d_ws = p;
+    running.push_back(r);
+    if (r->small) {
+      small.push_back(r);
+    } else {
+      next_stream = (next_stream + 1) % NSTREAMS;
+      launch_single(r);
+    }
+  }
+  if (!small.empty()) launch_batch(small);
+}
+
+void drtopk_server::loop() {
+  cudaSetDevice(device);
+  std::unique_lock<std::mutex> lk(mu);
+  while (true) {
+    if (stop && queue.empty() && running.empty()) break;
+    bool progressed = false;
+    for (auto it = running.begin(); it != running.end();) {
+      cudaError_t q = cudaEventQuery((*it)->ev);
+      if (q == cudaErrorNotReady) {
+        ++it;
+        continue;
+      }
+      Req* r = *it;
+      it = running.erase(it);
+      complete(r, q);
+      progressed = true;
+    }
+    const size_t before = queue.size();
+    if (!queue.empty()) admit_and_launch();
+    if (queue.size() != before) progressed = true;
+    if (progressed) done_cv.notify_all();
+    if (!progressed) {
+      if (running.empty() && queue.empty())
+        cv.wait_for(lk, std::chrono::milliseconds(5));
+      else
+        cv.wait_for(lk, std::chrono::microseconds(20));
+    }
+  }
+  done_cv.notify_all();
+}
+
+extern "C" drtopk_status_t drtopk_server_create(drtopk_server_t* out, int device, size_t hbm_budget_bytes,
+                                                int max_inflight) {
+  if (!out) return DRTOPK_EINVAL;
+  *out = nullptr;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cudaSetDevice(device) != cudaSuccess) return DRTOPK_EINVAL;
+  drtopk_server* s = new (std::nothrow) drtopk_server();
+  if (!s) return DRTOPK_ENOMEM;
+  s->device = device;
+  s->budget = hbm_budget_bytes;
+  s->max_inflight = max_inflight > 0 ? max_inflight : 64;
+  s->t0 = std::chrono::steady_clock::now();
+  drtopk_status_t st = drtopk_create(&s->h, device, 0);
+  for (int i = 0; st == DRTOPK_OK && i < NSTREAMS; ++i)
+    if (cudaStreamCreateWithFlags(&s->streams[i], cudaStreamNonBlocking) != cudaSuccess) st = DRTOPK_ECUDA;
+  if (st == DRTOPK_OK) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    if (segmented_shape(device, &s->seg_grid, &s->seg_smem) != cudaSuccess) st = DRTOPK_ECUDA;
+  }
+  cudaSetDevice(cur);
+  if (st != DRTOPK_OK) {
+    if (s->h) drtopk_destroy(s->h);
+    for (auto& x : s->streams)
+      if (x) cudaStreamDestroy(x);
+    delete s;
+    return st;
+  }
+  s->worker = std::thread([s]() { s->loop(); });
+  *out = s;
+  return DRTOPK_OK;
+}
+
+extern "C" drtopk_status_t drtopk_server_destroy(drtopk_server_t s) {
+  if (!s) return DRTOPK_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    // queued requests are cancelled
+    for (Req* r : s->queue) {
+      s->pinned.put(r->hkeys, r->hkeys_cap);
+      delete r;
+    }
+    s->queue.clear();
+  }
+  s->cv.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(s->device);
+  for (auto& x : s->streams)
+    if (x) cudaStreamSynchronize(x);
+  for (auto& x : s->streams)
+    if (x) cudaStreamDestroy(x);
+  for (auto e : s->ev_free) cudaEventDestroy(e);
+  s->pinned.clear();
+  drtopk_destroy(s->h);
+  cudaSetDevice(cur);
+  delete s;
+  return DRTOPK_OK;
+}
+
+static drtopk_status_t submit_impl(drtopk_server_t s, const void* h_keys, const void* d_keys, drtopk_dtype_t dtype,
+                                   uint64_t n, uint64_t k, int sorted, void* out_vals, int64_t* out_idx,
+                                   uint64_t* id) {
+  if (!s || (!h_keys && !d_keys) || n == 0 || k < 1 || k > n || n > 0xffffffffull) return DRTOPK_EINVAL;
+  if (dtype != DRTOPK_U32 && dtype != DRTOPK_F32) return DRTOPK_EINVAL;
+  Req* r = new (std::nothrow) Req();
+  if (!r) return DRTOPK_ENOMEM;
+  r->dtype = dtype;
+  r->n = n;
+  r->k = k;
+  r->sorted = sorted;
+  r->user_vals = out_vals;
+  r->user_idx = out_idx;
+  r->dkeys_user = d_keys;
+  r->small = n <= SMALL_N && k <= (uint64_t)SEG_MAX_K;
+  // coarse check here (the exact workspace is sized at admission, on the
+  // worker thread): the keys alone must fit the budget
+  if (s->budget && (d_keys ? 0 : n * 4) + k * 12 > s->budget) {
+    delete r;
+    return DRTOPK_EBUDGET;
+  }
+  if (h_keys) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->hkeys = s->pinned.get(n * 4, &r->hkeys_cap);
+    if (!r->hkeys) {
+      delete r;
+      return DRTOPK_ENOMEM;
+    }
+  }
+  if (h_keys) std::memcpy(r->hkeys, h_keys, n * 4);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->id = s->next_id++;
+    r->t_submit = s->now_ms();
+    s->queue.push_back(r);
+  }
+  if (id) *id = r->id;
+  s->cv.notify_all();
+  return DRTOPK_OK;
+}
+
+extern "C" drtopk_status_t drtopk_server_submit(drtopk_server_t s, const void* h_keys, drtopk_dtype_t dtype,
+                                                uint64_t n, uint64_t k, int sorted, void* out_vals, int64_t* out_idx,
+                                                uint64_t* id) {
+  if (!h_keys) return DRTOPK_EINVAL;
+  return submit_impl(s, h_keys, nullptr, dtype, n, k, sorted, out_vals, out_idx, id);
+}
+
+extern "C" drtopk_status_t drtopk_server_submit_device(drtopk_server_t s, const void* d_keys, drtopk_dtype_t dtype,
+                                                       uint64_t n, uint64_t k, int sorted, void* out_vals,
+                                                       int64_t* out_idx, uint64_t* id) {
+  if (!d_keys) return DRTOPK_EINVAL;
+  return submit_impl(s, nullptr, d_keys, dtype, n, k, sorted, out_vals, out_idx, id);
+}
+
+extern "C" drtopk_status_t drtopk_server_poll(drtopk_server_t s, drtopk_result_t* results, int max, int* count) {
+  if (!s || !count || (max > 0 && !results)) return DRTOPK_EINVAL;
+  std::lock_guard<std::mutex> lk(s->mu);
+  int c = 0;
+  while (c < max && !s->results.empty()) {
+    results[c++] = s->results.front();
+    s->results.pop_front();
+  }
+  *count = c;
+  return c ? DRTOPK_OK : DRTOPK_EAGAIN;
+}
+
+extern "C" drtopk_status_t drtopk_server_cancel(drtopk_server_t s, uint64_t id) {
+  if (!s) return DRTOPK_EINVAL;
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
+    if ((*it)->id == id) {
+      Req* r = *it;
+      s->queue.erase(it);
+      drtopk_result_t res;
+      std::memset(&res, 0, sizeof(res));
+      res.id = id;
+      res.status = DRTOPK_ECANCELLED;
+      res.t_submit_ms = r->t_submit;
+      res.t_done_ms = s->now_ms();
+      s->results.push_back(res);
+      s->pinned.put(r->hkeys, r->hkeys_cap);
+      delete r;
+      s->done_cv.notify_all();
+      return DRTOPK_OK;
+    }
+  }
+  return DRTOPK_EAGAIN;  // already started or unknown
+}
+
+extern "C" drtopk_status_t drtopk_server_drain(drtopk_server_t s, int timeout_ms) {
+  if (!s) return DRTOPK_EINVAL;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto pred = [&]() { return s->queue.empty() && s->running.empty(); };
+  if (timeout_ms < 0) {
+    s->done_cv.wait(lk, pred);
+    return DRTOPK_OK;
+  }
+  return s->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred) ? DRTOPK_OK : DRTOPK_ETIMEOUT;
+}
+
+extern "C" drtopk_status_t drtopk_server_usage(drtopk_server_t s, size_t* resident_bytes, int* inflight, int* queued) {
+  if (!s) return DRTOPK_EINVAL;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (resident_bytes) *resident_bytes = s->used;
+  if (inflight) *inflight = s->inflight;
+  if (queued) *queued = (int)s->queue.size();
+  return DRTOPK_OK;
+}

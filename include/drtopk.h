@@ -230,7 +230,13 @@ DRTOPK_API drtopk_status_t drtopk_server_destroy(drtopk_server_t s);
  * host buffers of k entries, filled when the request completes (may be NULL). */
 DRTOPK_API drtopk_status_t drtopk_server_submit(drtopk_server_t s, const void* h_keys, drtopk_dtype_t dtype, uint64_t n,
                                      uint64_t k, int sorted, void* out_vals, int64_t* out_idx, uint64_t* id);
-/* Pop up to max finished results; *count receives how many. */
+/* Same for keys already resident in device memory (caller-owned, left
+ * untouched until the request completes): no host copy, no upload. */
+DRTOPK_API drtopk_status_t drtopk_server_submit_device(drtopk_server_t s, const void* d_keys, drtopk_dtype_t dtype,
+                                                       uint64_t n, uint64_t k, int sorted, void* out_vals,
+                                                       int64_t* out_idx, uint64_t* id);
+/* Pop up to max finished results; *count receives how many (DRTOPK_EAGAIN
+ * when none has finished yet). */
 DRTOPK_API drtopk_status_t drtopk_server_poll(drtopk_server_t s, drtopk_result_t* results, int max, int* count);
 /* Cancel a request that has not started. */
 DRTOPK_API drtopk_status_t drtopk_server_cancel(drtopk_server_t s, uint64_t id);
