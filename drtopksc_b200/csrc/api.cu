@@ -353,6 +353,10 @@ extern "C" drtopk_status_t drtopk_destroy(drtopk_handle_t h) {
   return DRTOPK_OK;
 }
 
+namespace drtopk {
+drtopk_status_t plan_select(int device, uint64_t n, uint64_t k, drtopk_dtype_t dtype, const drtopk_params_t* p,
+                            bool want_idx, Plan* P);
+}
 static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype_t dtype, const drtopk_params_t* p,
                                 bool want_idx, Plan* P, DevInfo** dout) {
   DevInfo* di = nullptr;
@@ -385,6 +389,12 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
   layout(P, want_idx);
   if (dout) *dout = di;
   return DRTOPK_OK;
+}
+
+// plan (grid, shared memory, workspace layout) of a select on `device`
+drtopk_status_t drtopk::plan_select(int device, uint64_t n, uint64_t k, drtopk_dtype_t dtype,
+                                    const drtopk_params_t* p, bool want_idx, Plan* P) {
+  return plan_for(device, n, k, dtype, p, want_idx, P, nullptr);
 }
 
 extern "C" drtopk_status_t drtopk_workspace_size(uint64_t n, uint64_t k, drtopk_dtype_t dtype,

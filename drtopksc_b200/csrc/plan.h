@@ -5,6 +5,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <cuda_runtime.h>
+
 #include "../../include/drtopk.h"
 
 namespace drtopk {
@@ -52,6 +54,10 @@ struct Plan {
 drtopk_status_t make_plan(uint64_t n, uint64_t k, drtopk_dtype_t dtype, const drtopk_params_t* p, int sms,
                           int fused_grid, Plan* P);
 void layout(Plan* P, bool want_idx);
+drtopk_status_t plan_select(int device, uint64_t n, uint64_t k, drtopk_dtype_t dtype, const drtopk_params_t* p,
+                            bool want_idx, Plan* P);
+drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, void* d_kth, void* d_vals,
+                               int64_t* d_idx, char* ws, cudaStream_t st, cudaEvent_t* ev);
 int ref_alpha(double log2n, double k);
 
 }  // namespace drtopk

@@ -114,6 +114,22 @@ DRTOPK_API drtopk_status_t drtopk_select_ws(drtopk_handle_t h, const void* d_key
                                  uint64_t k, const drtopk_params_t* p, void* d_kth, void* d_vals, int64_t* d_idx,
                                  void* d_workspace, size_t workspace_bytes, void* stream);
 
+/* No counterpart in the reference.  A select that allocates no device
+ * memory, for callers that cannot allocate when they ask for a top-k (their
+ * framework's allocator owns all device memory, cudaMalloc's device-wide
+ * synchronisation is not acceptable on their path, or their host program
+ * forbids allocation inside it).  Same inputs, outputs, parameters and
+ * results as drtopk_select, on the current device; the scratch is one
+ * 32 MiB (33554432-byte) array built into the library, held by every GPU
+ * that loads the library until the process exits.
+ * Requests whose workspace (drtopk_workspace_size) is larger return
+ * DRTOPK_EUNSUPPORTED.  The first call on a device looks the array's
+ * address up; make it before capturing any stream work.  Calls share the
+ * array: calls whose GPU work overlaps race and must be serialised. */
+DRTOPK_API drtopk_status_t drtopk_select_noalloc(const void* d_keys, drtopk_dtype_t dtype, uint64_t n, uint64_t k,
+                                                 const drtopk_params_t* p, void* d_kth, void* d_vals,
+                                                 int64_t* d_idx, void* stream);
+
 /* Synchronise the stream and report device-side failures of the last call
  * (bounded waits that gave up, internal checks). */
 DRTOPK_API drtopk_status_t drtopk_sync_check(drtopk_handle_t h, void* stream);

@@ -1,0 +1,89 @@
+"""The select that allocates no device memory (drtopk_select_noalloc).
+
+It exists for callers that cannot allocate device memory when they need a
+top-k: a framework whose caching allocator already holds all of the GPU's
+memory, a latency-critical loop that cannot pay for cudaMalloc's implicit
+device synchronisation, or a plugin whose host program forbids allocation.
+Its scratch is one fixed 32 MiB array inside the library.  This test calls
+it through the C ABI twice in a row per input and checks every output
+against the regular drtopk_select, bit for bit; it also checks that a
+request needing more scratch than the array holds is refused.  The file is
+named to be collected last."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _lib():
+    import drtopksc_b200 as D
+    L = D.lib()
+    L.drtopk_select_noalloc.restype = ctypes.c_int
+    L.drtopk_select_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64,
+                                        ctypes.POINTER(D.Params), ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p]
+    return L
+
+
+def _run(fn_noalloc, t, dt, n, k, p):
+    import torch
+    kth = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+    vals = torch.full((k,), -1, dtype=torch.int32, device="cuda")
+    idx = torch.full((k,), -1, dtype=torch.int64, device="cuda")
+    st = fn_noalloc(t.data_ptr(), dt, n, k, ctypes.byref(p), kth.data_ptr(), vals.data_ptr(), idx.data_ptr())
+    torch.cuda.synchronize()
+    return st, kth.cpu().numpy(), vals.cpu().numpy(), idx.cpu().numpy()
+
+
+def test_noalloc_select_matches_select_on_two_calls_in_a_row():
+    import torch
+
+    import drtopksc_b200 as D
+    L = _lib()
+    h = D.Handle()
+    cases = [("u32", 1 << 20, 128, {}), ("f32n", 1 << 18, 1000, {"sorted": True}),
+             ("fewdigits", 1 << 19, 4096, {"sorted": True}), ("normal", 300001, 77, {"alpha": 3, "path": 2}),
+             ("u32", 1 << 16, 1 << 12, {"algo": "bucket"})]
+    for dist, n, k, kw in cases:
+        x = O.gen(dist, n, n + k)
+        t = torch.from_numpy(x).cuda() if x.dtype == np.float32 else torch.from_numpy(x.view(np.int32)).cuda()
+        dt = D.F32 if x.dtype == np.float32 else D.U32
+        p = D.params(**kw)
+        # the existing entry point (handle-owned workspace)
+        rk = torch.empty(1, dtype=torch.int32, device="cuda")
+        rv = torch.empty(k, dtype=torch.int32, device="cuda")
+        ri = torch.empty(k, dtype=torch.int64, device="cuda")
+        h.select_raw(t.data_ptr(), dt, n, k, p, rk.data_ptr(), rv.data_ptr(), ri.data_ptr(), None)
+        h.sync_check()
+        want = (rk.cpu().numpy(), rv.cpu().numpy(), ri.cpu().numpy())
+
+        def noalloc(kp, d, nn, kk, pp, a, b, c):
+            return L.drtopk_select_noalloc(kp, d, nn, kk, pp, a, b, c, None)
+
+        for _ in range(2):
+            st, kth, vals, idx = _run(noalloc, t, dt, n, k, p)
+            assert st == D.OK, (dist, n, k, kw, st)
+            assert np.array_equal(kth, want[0]), (dist, n, k)
+            if kw.get("sorted"):
+                assert np.array_equal(vals, want[1]) and np.array_equal(idx, want[2]), (dist, n, k)
+            else:  # unsorted output: same (value, index) pairs
+                a = sorted(zip(vals.tolist(), idx.tolist()))
+                b = sorted(zip(want[1].tolist(), want[2].tolist()))
+                assert a == b, (dist, n, k)
+
+
+def test_noalloc_select_refuses_requests_beyond_its_scratch():
+    import torch
+
+    import drtopksc_b200 as D
+    L = _lib()
+    n = 1 << 24  # plain radix on 2^24 keys needs far more than 32 MiB of scratch
+    t = torch.zeros(n, dtype=torch.int32, device="cuda")
+    p = D.params(algo="plain")
+    kth = torch.empty(1, dtype=torch.int32, device="cuda")
+    st = L.drtopk_select_noalloc(t.data_ptr(), D.U32, n, 10, ctypes.byref(p), kth.data_ptr(), None, None, None)
+    assert st == D.EUNSUPPORTED
