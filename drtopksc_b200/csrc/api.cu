@@ -66,6 +66,37 @@ static void* fused_ptr(int km) {
   }
 }
 
+template <int KM>
+static void* filter_fn() {
+  return (void*)k_filter<KM>;
+}
+template <int KM>
+static void* gather_fn() {
+  return (void*)k_gather<KM>;
+}
+static void* split_ptr(int km, bool filter) {
+  switch (km) {
+    case KM_U32: return filter ? filter_fn<KM_U32>() : gather_fn<KM_U32>();
+    case KM_F32: return filter ? filter_fn<KM_F32>() : gather_fn<KM_F32>();
+    case KM_U32_MIN: return filter ? filter_fn<KM_U32_MIN>() : gather_fn<KM_U32_MIN>();
+    default: return filter ? filter_fn<KM_F32_MIN>() : gather_fn<KM_F32_MIN>();
+  }
+}
+
+static cudaError_t split_grid(DevInfo* d, int km, bool filter, size_t smem, int* grid) {
+  static int occ_cache[64][4][2];
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  int& occ = occ_cache[d->device][km][filter ? 1 : 0];
+  if (occ == 0) {
+    int o = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, split_ptr(km, filter), FUSED_THREADS, smem);
+    if (e != cudaSuccess) return e;
+    occ = std::max(1, o);
+  }
+  *grid = occ * d->sms;
+  return cudaSuccess;
+}
+
 static cudaError_t fused_max_grid(DevInfo* d, int km, size_t smem, int* grid) {
   std::lock_guard<std::mutex> lk(g_dev_mu);
   if (d->occ_fused[km] == 0 || d->occ_fused_smem[km] != smem) {
@@ -380,6 +411,16 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
   // barrier participants)
   uint64_t want = std::max<uint64_t>((uint64_t)di->sms / 2, n >> 15);
   P->fused_grid = (int)std::min<uint64_t>((uint64_t)maxgrid, std::max<uint64_t>(1, want));
+  // split mode: the concatenation reads >= 16 MB (beta filter over >= 2^21
+  // subranges, or >= 2^22 keys re-read): run it as high-occupancy kernels
+  if (P->path == PATH_BETA || P->path == PATH_DEFAULT) {
+    const uint64_t concat = P->path == PATH_BETA ? P->M * 8 : k * P->S * 4;
+    P->split = concat >= (16ull << 20) ? 1 : 0;
+    const size_t hs = (size_t)std::max(P->nb, 256) * 4;
+    if (P->split && (split_grid(di, P->km, true, hs, &P->filter_grid) != cudaSuccess ||
+                     split_grid(di, P->km, false, hs, &P->split_grid) != cudaSuccess))
+      return DRTOPK_ECUDA;
+  }
   // sampler grid: persistent, capped by the work items
   if (P->path != PATH_PLAIN && !(P->path == PATH_BITONIC && P->normal)) {
     uint64_t items = P->alpha >= 9 ? P->M : ((n + 511) >> 9);
@@ -556,6 +597,9 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
   a.gb.gen = cw + CW_BAR_GEN;
   a.gb.err = cw + CW_ERR;
   a.gb.nblocks = (uint32_t)P.fused_grid;
+  a.thr_word = cw + CW_THR;
+  a.phase_lo = 1;
+  a.phase_hi = 3;
   a.out_kth = static_cast<uint32_t*>(d_kth);
   a.out_vals = static_cast<uint32_t*>(d_vals);
   a.out_idx = d_idx;
@@ -598,8 +642,32 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
     if (launch_sampler_km(P, sa, beta, st) != cudaSuccess) return DRTOPK_ECUDA;
   }
   if (ev) cudaEventRecord(ev[1], st);
-  // ---- fused cooperative kernel
-  drtopk_status_t s = launch_coop(fused_ptr(P.km), P, &a, st);
+  // ---- fused cooperative kernel (split mode: phase 1, concatenation kernels, phase 3)
+  drtopk_status_t s;
+  if (!P.split) {
+    s = launch_coop(fused_ptr(P.km), P, &a, st);
+  } else {
+    a.phase_hi = 1;
+    s = launch_coop(fused_ptr(P.km), P, &a, st);
+    const size_t smem = (size_t)std::max(P.nb, 256) * 4;
+    if (s == DRTOPK_OK && P.path == PATH_BETA) {
+      void* args[] = {&a};
+      if (cudaLaunchKernel(split_ptr(P.km, true), dim3(P.filter_grid), dim3(FUSED_THREADS), args, smem, st) !=
+          cudaSuccess)
+        s = DRTOPK_ECUDA;
+    }
+    if (s == DRTOPK_OK) {
+      void* args[] = {&a};
+      if (cudaLaunchKernel(split_ptr(P.km, false), dim3(P.split_grid), dim3(FUSED_THREADS), args, smem, st) !=
+          cudaSuccess)
+        s = DRTOPK_ECUDA;
+    }
+    if (s == DRTOPK_OK) {
+      a.phase_lo = 3;
+      a.phase_hi = 3;
+      s = launch_coop(fused_ptr(P.km), P, &a, st);
+    }
+  }
   if (ev) cudaEventRecord(ev[2], st);
   return s;
 }

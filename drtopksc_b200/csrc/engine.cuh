@@ -176,27 +176,33 @@ DRTOPK_DEV uint32_t src_key1(const Src& s, uint64_t i) {
   return s.raw_input ? to_key<KM>(v) : v;
 }
 
-// entry visitor over the source set (grid-stride, warp-uniform trip count).
-// fn(key, payload, valid) is called for every slot; valid=false for padding.
+// entry visitor over the source set: tiles of blockDim*16 entries per block
+// (16 independent coalesced loads in flight per thread), trip count uniform
+// per block.  fn(key, payload, valid) is called for every slot; valid=false
+// for padding.  Used by histogram passes (no appends inside fn).
 template <int KM, typename F>
 DRTOPK_DEV void for_each_src(const Src& s, bool from_pairs, uint64_t count, F&& fn) {
-  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t iters = (count + G - 1) / G;
-  for (uint64_t it = 0; it < iters; ++it) {
-    const uint64_t i = it * G + g;
-    const bool valid = i < count;
-    uint32_t key = 0, pay = 0;
-    if (valid) {
-      if (from_pairs) {
-        uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(s.pairs + i));
-        key = e.x; pay = e.y;
-      } else {
-        key = src_key1<KM>(s, i);
-        pay = (uint32_t)i;
+  constexpr int E = 16;
+  const uint64_t T = (uint64_t)blockDim.x * E;
+  for (uint64_t tb = (uint64_t)blockIdx.x * T; tb < count; tb += (uint64_t)gridDim.x * T) {
+    uint32_t key[E], pay[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const uint64_t i = tb + (uint64_t)e * blockDim.x + threadIdx.x;
+      key[e] = 0;
+      pay[e] = (uint32_t)i;
+      if (i < count) {
+        if (from_pairs) {
+          uint2 x = ld_cg_v2(reinterpret_cast<const uint32_t*>(s.pairs + i));
+          key[e] = x.x;
+          pay[e] = x.y;
+        } else {
+          key[e] = src_key1<KM>(s, i);
+        }
       }
     }
-    fn(key, pay, valid);
+#pragma unroll
+    for (int e = 0; e < E; ++e) fn(key[e], pay[e], tb + (uint64_t)e * blockDim.x + threadIdx.x < count);
   }
 }
 

@@ -64,6 +64,8 @@ struct FusedArgs {
   uint32_t* sort_cnt;     // [grid][256]
   uint32_t* sort_tot;     // [8][256]
   uint32_t* stats;        // [16]
+  uint32_t* thr_word;     // threshold handed between launches in split mode
+  int phase_lo, phase_hi; // phases run by this launch of k_fused (1..3)
   GridBar gb;
 };
 
@@ -103,7 +105,7 @@ DRTOPK_DEV void load4(const FusedArgs& a, uint64_t base, bool vec, uint32_t (&v)
 // block-aggregated append per tile.
 constexpr int GATHER_U = 8;
 
-template <int KM>
+template <int KM, int GATHER_U = drtopk::GATHER_U>
 DRTOPK_DEV void gather_list(const FusedArgs& a, const uint2* ids2, const uint32_t* ids1, uint64_t nsub, uint32_t thr,
                             uint32_t* s_hist, uint32_t& mlo, uint32_t& mhi, bool& ovf) {
   const uint64_t S = 1ull << a.alpha;
@@ -368,7 +370,9 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
   if (lead) stamp(a.stats, 16);
 
   // ---------------- phase 1: first select on the delegates
-  if (a.path == PATH_DEFAULT || a.path == PATH_BETA) {
+  if (a.phase_lo > 1) {
+    thr1 = ld_cg_u32(a.thr_word);
+  } else if (a.path == PATH_DEFAULT || a.path == PATH_BETA) {
     const uint64_t ndel = a.path == PATH_BETA ? 2 * a.M : a.M;
     Src s = {};
     s.keys = a.del;
@@ -402,12 +406,23 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
     }
   }
 
+  if (a.phase_lo <= 1 && lead) *a.thr_word = thr1;
+  if (a.phase_hi == 1) {
+    // split mode: the concatenation runs as separate kernels
+    if (lead) {
+      stamp(a.stats, 18);
+      a.stats[ST_LVA] = lvA;
+    }
+    return;
+  }
   // ---------------- phase 2: concatenation of candidates
-  if (lead) stamp(a.stats, 18);
+  if (lead && a.phase_lo <= 2) stamp(a.stats, 18);
   clear_hist(s_hist, a.nb);
   uint32_t mlo = 0, mhi = 0;
   bool ovf = false;
-  if (a.path == PATH_DEFAULT) {
+  if (a.phase_lo > 2) {
+    // concatenation already done by the split-mode kernels
+  } else if (a.path == PATH_DEFAULT) {
     // the k kept subranges must all be there before their ids are used as
     // addresses (every CTA reads the same count after the last barrier)
     if (ld_cg_u32(a.A.top_count) != a.k) {
@@ -430,7 +445,9 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
     gather_list<KM>(a, nullptr, a.sel, nsel_sub, thr1, s_hist, mlo, mhi, ovf);
   }
   if (ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
-  if (a.path != PATH_PLAIN) {
+  if (a.phase_lo > 2) {
+    // candidates' level-0 statistics were flushed by the split-mode kernels
+  } else if (a.path != PATH_PLAIN) {
     if (a.bucket) {
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
@@ -453,7 +470,10 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
   if (!grid_barrier(gb)) return;
 
   // ---------------- phase 3: second select
-  if (lead) stamp(a.stats, 20);
+  if (lead) {
+    stamp(a.stats, 20);
+    if (a.path == PATH_BETA && a.phase_lo > 2) a.stats[ST_NSEL] = ld_cg_u32(a.sel_count);
+  }
   Src sc = {};
   bool pairs;
   if (a.path == PATH_PLAIN) {
@@ -488,7 +508,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
     a.stats[ST_THR1] = thr1;
     if (a.path == PATH_DEFAULT) a.stats[ST_NSEL] = a.k;
     a.stats[ST_NCAND] = a.path == PATH_PLAIN ? (uint32_t)a.n : ld_cg_u32(a.cand_count);
-    a.stats[ST_LVA] = lvA;
+    if (a.phase_lo <= 1) a.stats[ST_LVA] = lvA;
     a.stats[ST_LVC] = rc.levels;
     a.stats[ST_TOPA] = a.path == PATH_DEFAULT ? ld_cg_u32(a.A.top_count) : 0u;
     a.stats[ST_TOPC] = ntop;
@@ -545,6 +565,67 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
     if (a.out_vals) a.out_vals[i] = from_key(~(uint32_t)(v >> 32), a.km);
     if (a.out_idx) a.out_idx[i] = (int64_t)(uint32_t)v;
   }
+}
+
+// --------------------------------------------------------------- split mode
+// For large concatenations the two streaming phases run as ordinary kernels
+// (many more resident warps than the cooperative kernel) between two
+// launches of k_fused (phase 1, then phase 3).  The threshold comes from
+// a.thr_word; counts are read after the kernel boundary.
+DRTOPK_DEV void flush_cand_stats(const FusedArgs& a, uint32_t* s_hist, uint32_t mlo, uint32_t mhi) {
+  if (a.bucket) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      mlo = max(mlo, __shfl_xor_sync(0xffffffffu, mlo, off));
+      mhi = max(mhi, __shfl_xor_sync(0xffffffffu, mhi, off));
+    }
+    if ((threadIdx.x & 31) == 0) { atomicMax(&a.cand_minmax[0], mlo); atomicMax(&a.cand_minmax[1], mhi); }
+  } else {
+    flush_hist(s_hist, a.C.H[0], a.nb);
+  }
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_filter(FusedArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  uint32_t* s_hist = s_dyn;
+  const uint32_t thr = ld_cg_u32(a.thr_word);
+  clear_hist(s_hist, a.nb);
+  uint32_t mlo = 0, mhi = 0;
+  bool ovf = false;
+  filter_beta<KM>(a, thr, s_hist, mlo, mhi, ovf);
+  if (ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
+  flush_cand_stats(a, s_hist, mlo, mhi);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_gather(FusedArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  uint32_t* s_hist = s_dyn;
+  const uint32_t thr = ld_cg_u32(a.thr_word);
+  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  uint64_t nsub;
+  if (a.path == PATH_DEFAULT) {
+    if (ld_cg_u32(a.A.top_count) != a.k) {  // uniform: written by the previous launch
+      if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
+      return;
+    }
+    nsub = a.k;
+  } else {
+    nsub = ld_cg_u32(a.sel_count);
+    if (nsub > a.M) {
+      if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
+      return;
+    }
+    if (lead) a.stats[ST_NLONELY] = ld_cg_u32(a.cand_count);  // lonely candidates came first
+  }
+  clear_hist(s_hist, a.nb);
+  uint32_t mlo = 0, mhi = 0;
+  bool ovf = false;
+  if (a.path == PATH_DEFAULT) gather_list<KM, 4>(a, a.A.top, nullptr, nsub, thr, s_hist, mlo, mhi, ovf);
+  else gather_list<KM, 4>(a, nullptr, a.sel, nsub, thr, s_hist, mlo, mhi, ovf);
+  if (ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
+  flush_cand_stats(a, s_hist, mlo, mhi);
 }
 
 }  // namespace drtopk

@@ -20,6 +20,7 @@ enum CtrlWord : int {
   CW_CAND_MINMAX = 6,  // 2 words
   CW_CAND_COUNT = 8,
   CW_SEL_COUNT = 9,
+  CW_THR = 10,         // first-select threshold handed between launches
   CW_STATS = 16,       // 32 words
   CTRL_HDR_WORDS = 48
 };
@@ -36,6 +37,8 @@ struct Plan {
   int sorted;
   uint64_t cand_cap;
   int fused_grid, sample_grid;
+  int split;           // concatenation as separate kernels (large inputs)
+  int split_grid, filter_grid;
   size_t fused_smem;
   size_t run_words;
   int hist_words;

@@ -4,11 +4,12 @@
 // budget allow (device memory from a stream-ordered pool, so admission never
 // synchronises the device), and keeps admitting while earlier requests are
 // still on the GPU:
-//   * large requests run one select each, round-robin over a ring of
-//     streams, so their copies and kernels overlap;
-//   * small requests (n <= 2^22, k <= 4096) admitted in the same tick are
-//     grouped into ONE persistent segmented launch (segmented.cuh), each
-//     segment reading and writing its request's own buffers.
+//   * requests with k <= 4096 admitted in the same tick are grouped into ONE
+//     persistent segmented launch (segmented.cuh), each segment reading and
+//     writing its request's own buffers; batches rotate over streams 1..7;
+//   * larger-k requests run one select each, in order on stream 0 (their
+//     fused kernel is a cooperative launch that wants the whole GPU, so
+//     they are pipelined rather than raced against each other).
 // Results are exact and identical to the plain call (same kernels / same
 // integer arithmetic); completion is detected with events and results are
 // copied into the caller's host buffers before they are reported by poll().
@@ -35,8 +36,7 @@ using namespace drtopk;
 
 namespace {
 
-constexpr int NSTREAMS = 8;
-constexpr uint64_t SMALL_N = 1ull << 22;
+constexpr int NSTREAMS = 8;  // stream 0: single selects (cooperative); 1..7: micro-batches
 
 struct Req {
   uint64_t id = 0;
@@ -69,10 +69,14 @@ struct Req {
   std::shared_ptr<int> batch_refs;
 };
 
+// Process-wide cache of pinned host buffers (size classes of powers of two),
+// shared by all servers so pinning happens once per process, not per request.
 struct PinnedCache {
+  std::mutex mu;
   std::multimap<size_t, void*> free_;
   size_t cached = 0;
   void* get(size_t bytes, size_t* cap) {
+    std::lock_guard<std::mutex> lk(mu);
     size_t c = 4096;
     while (c < bytes) c <<= 1;
     auto it = free_.lower_bound(c);
@@ -93,6 +97,7 @@ struct PinnedCache {
   }
   void put(void* p, size_t cap) {
     if (!p) return;
+    std::lock_guard<std::mutex> lk(mu);
     if (cached + cap > (size_t(8) << 30)) {
       cudaFreeHost(p);
       return;
@@ -100,12 +105,12 @@ struct PinnedCache {
     free_.emplace(cap, p);
     cached += cap;
   }
-  void clear() {
-    for (auto& kv : free_) cudaFreeHost(kv.second);
-    free_.clear();
-    cached = 0;
-  }
 };
+
+PinnedCache& pinned_cache() {
+  static PinnedCache* c = new PinnedCache();  // lives until process exit
+  return *c;
+}
 
 inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -131,7 +136,7 @@ struct drtopk_server {
   bool stop = false;
   std::thread worker;
   std::chrono::steady_clock::time_point t0;
-  PinnedCache pinned;
+  PinnedCache& pinned = pinned_cache();
   std::vector<cudaEvent_t> ev_free;
 
   double now_ms() const {
@@ -172,7 +177,7 @@ struct drtopk_server {
   void complete(Req* r, cudaError_t q);
   void admit_and_launch();
   void launch_single(Req* r);
-  void launch_batch(std::vector<Req*>& v);
+  void launch_batch(std::vector<Req*>& v, int si);
   void loop();
 };
 
@@ -225,10 +230,8 @@ void drtopk_server::launch_single(Req* r) {
   cudaEventRecord(r->ev, st);
 }
 
-void drtopk_server::launch_batch(std::vector<Req*>& v) {
-  const int si = next_stream;
+void drtopk_server::launch_batch(std::vector<Req*>& v, int si) {
   cudaStream_t st = streams[si];
-  next_stream = (next_stream + 1) % NSTREAMS;
   const int nseg = (int)v.size();
   std::vector<SegDesc> seg(nseg);
   std::vector<uint2> tasks;
@@ -336,6 +339,8 @@ void drtopk_server::admit_and_launch() {
   std::vector<Req*> small;
   int scanned = 0;
   const double t = now_ms();
+  // this tick's micro-batch stream: its requests' buffers are allocated on it
+  const int bs = 1 + next_stream % (NSTREAMS - 1);
   for (auto it = queue.begin(); it != queue.end() && inflight < max_inflight && scanned < 256; ++scanned) {
     Req* r = *it;
     size_t need = 0;
@@ -366,7 +371,7 @@ void drtopk_server::admit_and_launch() {
     r->ev = get_event();
     const size_t outb = al256(4) + al256(r->k * 4) + al256(r->k * 8);
     r->hout = pinned.get(outb, &r->hout_cap);
-    r->stream = next_stream;
+    r->stream = r->small ? bs : 0;
     cudaStream_t st = streams[r->stream];
     size_t dev = need;
     if (r->small) dev = (r->dkeys_user ? 0 : al256(r->n * 4)) + outb;  // batch workspace is separate
@@ -390,14 +395,13 @@ void drtopk_server::admit_and_launch() {
     p += al256(r->k * 8);
     r->d_ws = p;
     running.push_back(r);
-    if (r->small) {
-      small.push_back(r);
-    } else {
-      next_stream = (next_stream + 1) % NSTREAMS;
-      launch_single(r);
-    }
+    if (r->small) small.push_back(r);
+    else launch_single(r);
   }
-  if (!small.empty()) launch_batch(small);
+  if (!small.empty()) {
+    launch_batch(small, bs);
+    next_stream = (next_stream + 1) % (NSTREAMS - 1);
+  }
 }
 
 void drtopk_server::loop() {
@@ -490,7 +494,6 @@ extern "C" drtopk_status_t drtopk_server_destroy(drtopk_server_t s) {
   for (auto& x : s->streams)
     if (x) cudaStreamDestroy(x);
   for (auto e : s->ev_free) cudaEventDestroy(e);
-  s->pinned.clear();
   drtopk_destroy(s->h);
   cudaSetDevice(cur);
   delete s;
@@ -511,7 +514,7 @@ static drtopk_status_t submit_impl(drtopk_server_t s, const void* h_keys, const 
   r->user_vals = out_vals;
   r->user_idx = out_idx;
   r->dkeys_user = d_keys;
-  r->small = n <= SMALL_N && k <= (uint64_t)SEG_MAX_K;
+  r->small = k <= (uint64_t)SEG_MAX_K;  // micro-batched through the segmented kernel
   // coarse check here (the exact workspace is sized at admission, on the
   // worker thread): the keys alone must fit the budget
   if (s->budget && (d_keys ? 0 : n * 4) + k * 12 > s->budget) {
@@ -519,7 +522,6 @@ static drtopk_status_t submit_impl(drtopk_server_t s, const void* h_keys, const 
     return DRTOPK_EBUDGET;
   }
   if (h_keys) {
-    std::lock_guard<std::mutex> lk(s->mu);
     r->hkeys = s->pinned.get(n * 4, &r->hkeys_cap);
     if (!r->hkeys) {
       delete r;

@@ -354,3 +354,16 @@ def test_sampler_delegates_every_alpha(alpha):
         else:
             assert np.array_equal(dl, O.sample_top2(x, alpha)), alpha
         assert kth == O.topk_exact(x, k, False)[0]
+
+
+@pytest.mark.parametrize("dist,n,k,alpha,path", [
+    ("u32", 1 << 23, 1 << 14, 2, 2), ("normal", 1 << 23, 1 << 16, 6, 1), ("f32n", 1 << 23, 5000, 1, 2),
+    ("fewdigits", 1 << 22, 3000, 1, 2)])
+def test_split_mode_large_concatenation(dist, n, k, alpha, path):
+    """Concatenations of >= 16 MB run as separate filter/gather kernels between
+    two launches of the fused kernel; results must not change."""
+    x = O.gen(dist, n, n + k)
+    st = check_exact(x, k, alpha=alpha, path=path)
+    _, ost = O.radix_final_kth(x, k, 8, alpha=alpha, path=path)
+    assert st["first_threshold"] == ost["first_flag"]
+    assert st["n_selected"] == ost["n_selected"]
