@@ -438,6 +438,8 @@ def main():
         out = {}
         for i, k in enumerate(ks):
             pk = params_for(i, k)
+            # one untimed call (sizes the workspace for this configuration)
+            h.select_raw(keys.data_ptr(), D.U32, n, k, pk, kth.data_ptr() + 4 * i, vals.data_ptr(), None, sp)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             reps = 3
             a.record(stream)

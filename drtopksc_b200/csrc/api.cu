@@ -101,7 +101,9 @@ static cudaError_t fused_max_grid(DevInfo* d, int km, size_t smem, int* grid) {
   std::lock_guard<std::mutex> lk(g_dev_mu);
   if (d->occ_fused[km] == 0 || d->occ_fused_smem[km] != smem) {
     int occ = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_ptr(km), FUSED_THREADS, smem);
+    cudaError_t e = cudaFuncSetAttribute(fused_ptr(km), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_ptr(km), FUSED_THREADS, smem);
     if (e != cudaSuccess) return e;
     d->occ_fused[km] = std::max(1, occ);
     d->occ_fused_smem[km] = smem;
@@ -260,7 +262,7 @@ void layout(Plan* P, bool want_idx) {
   // each run's histograms hold max(nb, 256) bins: the tie-fill sub-run
   // always uses 8-bit digits even when the bucket variant has fewer buckets
   P->hist_words = std::max(P->nb, 256);
-  P->run_words = 3 * P->hist_words + (MAX_LEVELS + 2) + 1;
+  P->run_words = 3 * P->hist_words + (MAX_LEVELS + 2) + 1 + 4;
   size_t ctrl_words = CTRL_HDR_WORDS + 4 * (size_t)P->run_words + 8 * 256;
   P->off_ctrl = take(ctrl_words * 4);
   P->ctrl_bytes = ctrl_words * 4;
@@ -394,8 +396,9 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
   if (dev_info(device, &di) != cudaSuccess) return DRTOPK_ECUDA;
   drtopk_status_t s = make_plan(n, k, dtype, p, di->sms, 0, P);
   if (s != DRTOPK_OK) return s;
-  // dynamic shared memory of the fused kernel
-  size_t smem = (size_t)std::max(P->nb, 256) * 4;
+  // dynamic shared memory of the fused kernel: histogram + two SMALL_SET
+  // buffers for runs finished in one CTA (or the small top-k sort)
+  size_t smem = (size_t)((std::max(P->nb, 256) + 3) & ~3) * 4 + 2 * (size_t)SMALL_SET * 8;
   if (P->sorted && k <= (uint64_t)SMALL_SORT) {
     size_t np2 = 1;
     while (np2 < k) np2 <<= 1;
@@ -486,6 +489,7 @@ static RunBufs run_bufs(char* ctrl, const Plan& P, int which) {
   r.H[2] = base + 2 * P.hist_words;
   r.set_count = base + 3 * P.hist_words;
   r.top_count = base + 3 * P.hist_words + MAX_LEVELS + 2;
+  r.res = base + 3 * P.hist_words + MAX_LEVELS + 2 + 1;
   r.cbuf[0] = r.cbuf[1] = nullptr;
   r.top = nullptr;
   return r;
@@ -853,7 +857,9 @@ extern "C" drtopk_status_t drtopk_profile_end(drtopk_handle_t h, double* ms_samp
 //                                 + 4kS (the k kept subranges re-read)
 //   two delegates (beta path):    8M (write) + 8M per extra threshold digit
 //                                 + 8M (filter read) + 4S per subrange with
-//                                 >= 2 keys above the threshold + 8 per
+//                                 >= 2 keys above the threshold (scattered
+//                                 subrange reads, weighted x2 against
+//                                 streaming bytes as measured) + 8 per
 //                                 candidate; a threshold of d digits admits
 //                                 an extra ~2^-8d of the keys (truncation).
 // Subrange counts per bucket follow Poisson(lambda = q' S).
@@ -869,7 +875,7 @@ static double cost_beta(double n, double k, double S, int digits) {
   const double p_sel = 1.0 - e * (1.0 + lam);
   const double p_lone = lam * e;
   const double cand = M * p_lone + M * p_sel * (lam + 1.0);
-  return 16.0 * M + 8.0 * M * (digits - 1) + M * p_sel * 4.0 * S + 24.0 * cand;
+  return 16.0 * M + 8.0 * M * (digits - 1) + 2.0 * M * p_sel * 4.0 * S + 24.0 * cand;
 }
 
 extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_t dtype, drtopk_params_t* p) {

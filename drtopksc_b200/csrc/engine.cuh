@@ -28,6 +28,8 @@ namespace drtopk {
 constexpr int FUSED_THREADS = 256;
 constexpr int MAX_LEVELS = 40;
 
+constexpr int SMALL_SET = 4096;  // a set this small is finished by one CTA in shared memory
+
 struct EngineCfg {
   int bucket;          // 0 radix, 1 bucket
   int nbits;           // radix digit width
@@ -44,6 +46,7 @@ struct RunBufs {
   uint2* cbuf[2];       // compact ping-pong buffers
   uint2* top;           // top list (capacity k)
   uint32_t* top_count;
+  uint32_t* res;        // [4] result of a run finished inside one CTA: thr, kth, levels, ok
 };
 
 struct Level {
@@ -81,6 +84,8 @@ struct Pick {
 };
 
 // Every CTA: find the largest bin b with (count of bins >= b) >= R.
+// H in global memory (written by other CTAs) or, with SMEM, shared memory.
+template <bool SMEM = false>
 DRTOPK_DEV Pick block_pick(const uint32_t* H, int nb, uint32_t R) {
   __shared__ uint32_t s_part[FUSED_THREADS / 32];
   __shared__ Pick s_pick;
@@ -88,8 +93,9 @@ DRTOPK_DEV Pick block_pick(const uint32_t* H, int nb, uint32_t R) {
   const int t = threadIdx.x;
   const int q = (nb + FUSED_THREADS - 1) / FUSED_THREADS;
   const int b0 = min(nb, t * q), b1 = min(nb, b0 + q);
+  auto hb = [&](int b) { return SMEM ? H[b] : ld_cg_u32(H + b); };
   uint32_t local = 0;
-  for (int b = b0; b < b1; ++b) local += ld_cg_u32(H + b);
+  for (int b = b0; b < b1; ++b) local += hb(b);
   // inclusive prefix over threads (ascending), then above_t = total - incl
   uint32_t incl = local;
   const unsigned lane = t & 31u;
@@ -111,7 +117,7 @@ DRTOPK_DEV Pick block_pick(const uint32_t* H, int nb, uint32_t R) {
   if (local > 0 && above_t < R && R <= above_t + local) {
     uint32_t acc = above_t;
     for (int b = b1 - 1; b >= b0; --b) {
-      uint32_t c = ld_cg_u32(H + b);
+      uint32_t c = hb(b);
       if (acc + c >= R) {
         s_pick.b = b; s_pick.cnt = c; s_pick.above = acc;
         s_found = 1;
@@ -124,7 +130,7 @@ DRTOPK_DEV Pick block_pick(const uint32_t* H, int nb, uint32_t R) {
   Pick p;
   if (s_found) p = s_pick;
   else {  // R exceeds the set: the reference's rule then picks bin 0
-    uint32_t h0 = ld_cg_u32(H);
+    uint32_t h0 = hb(0);
     p.b = 0; p.cnt = h0; p.above = total - h0;
   }
   __syncthreads();
@@ -268,12 +274,13 @@ DRTOPK_DEV void split_tiles(const EngineCfg& c, const Src& s, bool pairs, uint64
 template <int KM>
 DRTOPK_DEV int run_levels(const EngineCfg& c, const Src& src0, bool src0_pairs, const RunBufs& rb, Level L,
                           uint32_t* s_hist, const GridBar& gb, Level& Lout, Pick& last_pick, int& eq_buf,
-                          uint64_t& eq_count, bool& ok) {
+                          uint64_t& eq_count, bool& ok, bool small_exit = false, bool* went_small = nullptr) {
   int j = 0;
   ok = true;
+  if (went_small) *went_small = false;
   for (;; ++j) {
     if (j >= MAX_LEVELS) { ok = false; break; }
-    Pick p = block_pick(rb.H[j % 3], c.nb, L.R);
+    Pick p = block_pick<false>(rb.H[j % 3], c.nb, L.R);
     Level N;
     bool done = advance(c, L, p, j, N);
     last_pick = p;
@@ -314,8 +321,108 @@ DRTOPK_DEV int run_levels(const EngineCfg& c, const Src& src0, bool src0_pairs, 
       eq_count = ld_cg_u32(rb.set_count + j + 1);
       break;
     }
+    if (small_exit && ld_cg_u32(rb.set_count + j + 1) <= (uint32_t)SMALL_SET) {
+      // the next set fits one CTA's shared memory: finish there
+      Lout = N;
+      eq_buf = j & 1;
+      eq_count = ld_cg_u32(rb.set_count + j + 1);
+      *went_small = true;
+      break;
+    }
   }
   return j;
+}
+
+// ascending bitonic sort of npow2 64-bit values in shared memory (one CTA)
+DRTOPK_DEV void block_bitonic_asc(uint64_t* s, int npow2) {
+  for (int size = 2; size <= npow2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < npow2 / 2; i += blockDim.x) {
+        const int lo = 2 * stride * (i / stride) + (i % stride), hi = lo + stride;
+        const bool asc = ((lo & size) == 0);
+        const uint64_t x = s[lo], y = s[hi];
+        if ((x > y) == asc) { s[lo] = y; s[hi] = x; }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Completion of a run inside ONE CTA once its remaining set (cnt <=
+// SMALL_SET entries) fits in shared memory: the same levels (pick /
+// advance / split), then the tie fill by lowest payload, with block
+// barriers only.  Results go to rb.top (global, after the entries already
+// there) and rb.res.  Called by all threads of one CTA.
+template <int KM>
+DRTOPK_DEV void block_finish(const EngineCfg& c, const Src& src, bool pairs, uint32_t cnt, Level L, int j,
+                             const RunBufs& rb, uint32_t* s_hist, uint2* sA, uint2* sB) {
+  __shared__ uint32_t s_n;
+  for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+    if (pairs) sA[i] = ld_cg_v2(reinterpret_cast<const uint32_t*>(src.pairs + i));
+    else sA[i] = make_uint2(src_key1<KM>(src, i), i);
+  }
+  uint32_t n = cnt;
+  bool ok = true;
+  for (;;) {
+    if (j >= MAX_LEVELS) { ok = false; break; }
+    clear_hist(s_hist, c.nb);
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+      atomicAdd(&s_hist[bin_of(sA[i].x, L.lo, L.w, L.wshift)], 1u);
+    __syncthreads();
+    const Pick p = block_pick<true>(s_hist, c.nb, L.R);
+    Level N;
+    const bool done = advance(c, L, p, j, N);
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < n; base += blockDim.x) {
+      const uint32_t i = base + threadIdx.x;
+      const uint2 e = i < n ? sA[i] : make_uint2(0u, 0u);
+      const bool up = i < n && e.x > N.hi;
+      const bool in = i < n && e.x >= N.lo && e.x <= N.hi;
+      const uint32_t s1 = block_append1(up, rb.top_count);
+      if (up) rb.top[s1] = e;
+      const uint32_t s2 = block_append1(in, &s_n);
+      if (in) sB[s2] = e;
+    }
+    __syncthreads();
+    n = s_n;
+    uint2* t = sA; sA = sB; sB = t;
+    L = N;
+    ++j;
+    if (done) break;
+  }
+  const uint32_t R = L.R;
+  const uint32_t kth = (n == 1) ? sA[0].x : L.lo;
+  if (ok && n == R) {
+    for (uint32_t base = 0; base < n; base += blockDim.x) {
+      const uint32_t i = base + threadIdx.x;
+      const uint32_t s1 = block_append1(i < n, rb.top_count);
+      if (i < n) rb.top[s1] = sA[i];
+    }
+  } else if (ok && n > R) {
+    // keep the R lowest payloads among the tied entries
+    uint64_t* w = reinterpret_cast<uint64_t*>(sB);
+    int np2 = 1;
+    while (np2 < (int)n) np2 <<= 1;
+    for (int i = threadIdx.x; i < np2; i += blockDim.x)
+      w[i] = i < (int)n ? (((uint64_t)sA[i].y << 32) | sA[i].x) : ~0ull;
+    block_bitonic_asc(w, np2);
+    for (uint32_t base = 0; base < R; base += blockDim.x) {
+      const uint32_t i = base + threadIdx.x;
+      const uint32_t s1 = block_append1(i < R, rb.top_count);
+      if (i < R) rb.top[s1] = make_uint2((uint32_t)w[i], (uint32_t)(w[i] >> 32));
+    }
+  } else {
+    ok = false;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    rb.res[0] = L.lo;
+    rb.res[1] = kth;
+    rb.res[2] = (uint32_t)j;
+    rb.res[3] = ok ? 1u : 0u;
+  }
 }
 
 // histogram pass of level 0 for a run: hist of bin_of(key, L0) over the source
@@ -351,18 +458,41 @@ DRTOPK_DEV Level bucket_level0(uint32_t mn, uint32_t mx, int nb, uint32_t R) {
 // compact buffers alias rb's).
 template <int KM>
 DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_pairs, const RunBufs& rb,
-                                const RunBufs& fb, Level L0, uint32_t* s_hist, const GridBar& gb) {
+                                const RunBufs& fb, Level L0, uint32_t* s_hist, const GridBar& gb,
+                                uint2* s_fast = nullptr) {
   RunResult res = {0u, 0u, 0, 1};
+  const bool can_small = s_fast && !c.thr_only && !c.key_from_payload;
+  auto finish_small = [&](const Src& s, bool pairs, uint32_t cnt, const Level& L, int j0) {
+    if (blockIdx.x == 0) block_finish<KM>(c, s, pairs, cnt, L, j0, rb, s_hist, s_fast, s_fast + SMALL_SET);
+    if (!grid_barrier(gb)) { res.ok = 0; return; }
+    res.thr = ld_cg_u32(rb.res);
+    res.kth = ld_cg_u32(rb.res + 1);
+    res.levels = (int)ld_cg_u32(rb.res + 2);
+    res.ok = ld_cg_u32(rb.res + 3) ? 1 : 0;
+  };
+  if (can_small) {
+    const uint64_t n0 = src0_pairs ? (uint64_t)ld_cg_u32(src0.count_dev) : src0.count;
+    if (n0 <= (uint64_t)SMALL_SET) {
+      finish_small(src0, src0_pairs, (uint32_t)n0, L0, 0);
+      return res;
+    }
+  }
   Level Lf;
   Pick lp;
   int eqb = 0;
   uint64_t E = 0;
-  bool ok = true;
-  int j = run_levels<KM>(c, src0, src0_pairs, rb, L0, s_hist, gb, Lf, lp, eqb, E, ok);
+  bool ok = true, small = false;
+  int j = run_levels<KM>(c, src0, src0_pairs, rb, L0, s_hist, gb, Lf, lp, eqb, E, ok, can_small, &small);
   res.levels = j + 1;
   res.thr = Lf.lo;
   if (!ok) { res.ok = 0; return res; }
   if (c.thr_only) return res;
+  if (small) {
+    Src s = {};
+    s.pairs = rb.cbuf[eqb];
+    finish_small(s, true, (uint32_t)E, Lf, j + 1);
+    return res;
+  }
   const uint2* eq = rb.cbuf[eqb];
   res.kth = (E == 1) ? ld_cg_v2(reinterpret_cast<const uint32_t*>(eq)).x : Lf.lo;
   const uint32_t R = Lf.R;

@@ -362,6 +362,8 @@ template <int KM>
 __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
   extern __shared__ __align__(16) uint32_t s_dyn[];
   uint32_t* s_hist = s_dyn;
+  // two SMALL_SET-entry buffers after the histogram (runs finished in one CTA)
+  uint2* s_fast = reinterpret_cast<uint2*>(s_dyn + ((max(a.nb, 256) + 3) & ~3));
   const GridBar& gb = a.gb;
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   const int D = 32 / a.nbits;
@@ -397,7 +399,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
     if (a.path == PATH_BETA && c.max_levels <= 0) {
       thr1 = 0;  // no digit processed: every subrange qualifies
     } else {
-      RunResult r = run_select<KM>(c, s, false, a.A, a.AF, L0, s_hist, gb);
+      RunResult r = run_select<KM>(c, s, false, a.A, a.AF, L0, s_hist, gb, s_fast);
       if (!r.ok) { if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL); return; }
       lvA = r.levels;
       // radix keeps the reference's flag (final range lower bound); the bucket
@@ -498,7 +500,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
   EngineCfg cc;
   cc.bucket = a.bucket; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
   cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0;
-  RunResult rc = run_select<KM>(cc, sc, pairs, a.C, a.CF, L0c, s_hist, gb);
+  RunResult rc = run_select<KM>(cc, sc, pairs, a.C, a.CF, L0c, s_hist, gb, s_fast);
   if (!rc.ok) { if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL); return; }
   const uint32_t K = rc.kth;
   const uint32_t ntop = ld_cg_u32(a.C.top_count);
