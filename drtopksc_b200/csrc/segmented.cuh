@@ -94,14 +94,24 @@ DRTOPK_DEV void seg_sample_chunk(const SegArgs& a, const SegDesc& d, uint32_t ch
   for (uint64_t j = (c0 >> alpha) + wid; j < ((c1 + S - 1) >> alpha); j += nw) {
     const uint64_t b = j << alpha, e = min(len, b + S);
     uint32_t m = 0;
-    for (uint64_t p = b + lane * 4; p < e; p += 128) {
-      if (vec && p + 4 <= e) {
-        uint4 v = __ldg(reinterpret_cast<const uint4*>(keys + p));
-        m = max(max(m, max(to_key_rt(v.x, d.km), to_key_rt(v.y, d.km))),
-                max(to_key_rt(v.z, d.km), to_key_rt(v.w, d.km)));
-      } else {
-        for (int q = 0; q < 4; ++q)
-          if (p + q < e) m = max(m, to_key_rt(__ldg(keys + p + q), d.km));
+    for (uint64_t p0 = b + lane * 4; p0 < e; p0 += 512) {
+      uint4 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint64_t p = p0 + 128 * u;
+        if (vec && p + 4 <= e) v[u] = __ldg(reinterpret_cast<const uint4*>(keys + p));
+        else {
+          uint32_t t[4];
+          for (int q = 0; q < 4; ++q) t[q] = (p + q < e) ? __ldg(keys + p + q) : 0u;
+          v[u] = make_uint4(t[0], t[1], t[2], t[3]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint64_t p = p0 + 128 * u;
+        const uint32_t x0 = p < e ? to_key_rt(v[u].x, d.km) : 0u, x1 = p + 1 < e ? to_key_rt(v[u].y, d.km) : 0u;
+        const uint32_t x2 = p + 2 < e ? to_key_rt(v[u].z, d.km) : 0u, x3 = p + 3 < e ? to_key_rt(v[u].w, d.km) : 0u;
+        m = max(m, max(max(x0, x1), max(x2, x3)));
       }
     }
     m = __reduce_max_sync(0xffffffffu, m);
@@ -122,9 +132,19 @@ DRTOPK_DEV uint32_t block_kth(uint64_t n, uint32_t k, G&& get, uint32_t* s_hist,
     const uint32_t mask_hi = (d == 3) ? 0u : (0xffffffffu << (sh + 8));
     for (int i = threadIdx.x; i < 256; i += blockDim.x) s_hist[i] = 0;
     __syncthreads();
-    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
-      const uint32_t v = get(i);
-      if ((v & mask_hi) == lo) atomicAdd(&s_hist[(v >> sh) & 255u], 1u);
+    constexpr int U = 8;  // independent loads in flight per thread
+    for (uint64_t b = 0; b < n; b += (uint64_t)blockDim.x * U) {
+      uint32_t v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const uint64_t i = b + (uint64_t)u * blockDim.x + threadIdx.x;
+        v[u] = i < n ? get(i) : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const uint64_t i = b + (uint64_t)u * blockDim.x + threadIdx.x;
+        if (i < n && (v[u] & mask_hi) == lo) atomicAdd(&s_hist[(v[u] >> sh) & 255u], 1u);
+      }
     }
     __syncthreads();
     if (threadIdx.x < 32) {
@@ -165,32 +185,41 @@ DRTOPK_DEV uint32_t block_ordered_take(uint64_t n, uint32_t K, uint32_t need_eq,
   if (threadIdx.x == 0) { s_run[0] = 0; s_run[1] = 0; }
   __syncthreads();
   const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-  for (uint64_t base = 0; base < n; base += blockDim.x) {
-    const uint64_t i = base + threadIdx.x;
-    uint32_t v = 0;
-    const bool valid = i < n;
-    if (valid) v = get(i);
-    const bool gt = valid && v > K, eq = valid && v == K;
-    const unsigned bg = __ballot_sync(0xffffffffu, gt), be = __ballot_sync(0xffffffffu, eq);
-    if (lane == 0) { s_w[0][wid] = __popc(bg); s_w[1][wid] = __popc(be); }
-    __syncthreads();
-    uint32_t pg = 0, pe = 0, tg = 0, te = 0;
-    for (int w = 0; w < SEG_THREADS / 32; ++w) {
-      if (w < (int)wid) { pg += s_w[0][w]; pe += s_w[1][w]; }
-      tg += s_w[0][w];
-      te += s_w[1][w];
+  constexpr int U = 4;  // loads issued together; ranked one sub-round at a time (index order)
+  for (uint64_t base = 0; base < n; base += (uint64_t)blockDim.x * U) {
+    uint32_t vv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint64_t i = base + (uint64_t)u * blockDim.x + threadIdx.x;
+      vv[u] = i < n ? get(i) : 0u;
     }
-    const uint32_t lm = (1u << lane) - 1u;
-    const uint32_t rg = s_run[0] + pg + __popc(bg & lm);   // rank among > K so far
-    const uint32_t re = s_run[1] + pe + __popc(be & lm);   // rank among == K so far
-    const bool take_eq = eq && re < need_eq;
-    // slots: all > K and the taken == K, interleaved in index order
-    const uint32_t eq_before = min(re, need_eq);
-    if (gt) emit(rg + eq_before, i);
-    if (take_eq) emit(rg + re, i);
-    __syncthreads();
-    if (threadIdx.x == 0) { s_run[0] += tg; s_run[1] += te; }
-    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint64_t i = base + (uint64_t)u * blockDim.x + threadIdx.x;
+      const uint32_t v = vv[u];
+      const bool valid = i < n;
+      const bool gt = valid && v > K, eq = valid && v == K;
+      const unsigned bg = __ballot_sync(0xffffffffu, gt), be = __ballot_sync(0xffffffffu, eq);
+      if (lane == 0) { s_w[0][wid] = __popc(bg); s_w[1][wid] = __popc(be); }
+      __syncthreads();
+      uint32_t pg = 0, pe = 0, tg = 0, te = 0;
+      for (int w = 0; w < SEG_THREADS / 32; ++w) {
+        if (w < (int)wid) { pg += s_w[0][w]; pe += s_w[1][w]; }
+        tg += s_w[0][w];
+        te += s_w[1][w];
+      }
+      const uint32_t lm = (1u << lane) - 1u;
+      const uint32_t rg = s_run[0] + pg + __popc(bg & lm);   // rank among > K so far
+      const uint32_t re = s_run[1] + pe + __popc(be & lm);   // rank among == K so far
+      const bool take_eq = eq && re < need_eq;
+      // slots: all > K and the taken == K, interleaved in index order
+      const uint32_t eq_before = min(re, need_eq);
+      if (gt) emit(rg + eq_before, i);
+      if (take_eq) emit(rg + re, i);
+      __syncthreads();
+      if (threadIdx.x == 0) { s_run[0] += tg; s_run[1] += te; }
+      __syncthreads();
+    }
   }
   const uint32_t kept = s_run[0] + min(s_run[1], need_eq);
   __syncthreads();

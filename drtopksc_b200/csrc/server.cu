@@ -4,10 +4,10 @@
 // budget allow (device memory from a stream-ordered pool, so admission never
 // synchronises the device), and keeps admitting while earlier requests are
 // still on the GPU:
-//   * requests with k <= 4096 admitted in the same tick are grouped into ONE
+//   * requests with n <= 2^22 and k <= 4096 admitted in the same tick are grouped into ONE
 //     persistent segmented launch (segmented.cuh), each segment reading and
 //     writing its request's own buffers; batches rotate over streams 1..7;
-//   * larger-k requests run one select each, in order on stream 0 (their
+//   * other requests run one select each, in order on stream 0 (their
 //     fused kernel is a cooperative launch that wants the whole GPU, so
 //     they are pipelined rather than raced against each other).
 // Results are exact and identical to the plain call (same kernels / same
@@ -37,6 +37,7 @@ using namespace drtopk;
 namespace {
 
 constexpr int NSTREAMS = 8;  // stream 0: single selects (cooperative); 1..7: micro-batches
+constexpr uint64_t BATCH_MAX_N = 1ull << 22;  // larger inputs run as single selects
 
 struct Req {
   uint64_t id = 0;
@@ -514,7 +515,7 @@ static drtopk_status_t submit_impl(drtopk_server_t s, const void* h_keys, const 
   r->user_vals = out_vals;
   r->user_idx = out_idx;
   r->dkeys_user = d_keys;
-  r->small = k <= (uint64_t)SEG_MAX_K;  // micro-batched through the segmented kernel
+  r->small = n <= BATCH_MAX_N && k <= (uint64_t)SEG_MAX_K;  // micro-batched through the segmented kernel
   // coarse check here (the exact workspace is sized at admission, on the
   // worker thread): the keys alone must fit the budget
   if (s->budget && (d_keys ? 0 : n * 4) + k * 12 > s->budget) {
