@@ -45,7 +45,7 @@ class DrTopKError(RuntimeError):
 class Params(ctypes.Structure):
     _fields_ = [("nbits", ctypes.c_int), ("alpha", ctypes.c_int), ("beta", ctypes.c_int), ("path", ctypes.c_int),
                 ("algo", ctypes.c_int), ("num_bucket", ctypes.c_int), ("largest", ctypes.c_int),
-                ("sorted", ctypes.c_int), ("first_digits", ctypes.c_int)]
+                ("sorted", ctypes.c_int), ("first_digits", ctypes.c_int), ("team", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -54,10 +54,18 @@ class Stats(ctypes.Structure):
                 ("n_selected", ctypes.c_uint64), ("n_lonely", ctypes.c_uint64), ("n_candidates", ctypes.c_uint64),
                 ("levels_first", ctypes.c_int), ("levels_second", ctypes.c_int), ("device_error", ctypes.c_uint32),
                 ("ms_sample", ctypes.c_double), ("ms_first", ctypes.c_double), ("ms_concat", ctypes.c_double),
-                ("ms_second", ctypes.c_double), ("ms_total", ctypes.c_double)]
+                ("ms_second", ctypes.c_double), ("ms_total", ctypes.c_double), ("team_ctas", ctypes.c_int),
+                ("team_cluster", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("singles", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("batched", ctypes.c_uint64),
+                ("pinned_allocs", ctypes.c_uint64), ("worker_ticks", ctypes.c_uint64),
+                ("host_ms_pinned", ctypes.c_double), ("host_ms_launch", ctypes.c_double),
+                ("host_ms_complete", ctypes.c_double)]
 
 
 class Result(ctypes.Structure):
@@ -117,6 +125,7 @@ def lib() -> ctypes.CDLL:
             "drtopk_server_cancel": (st, [vp, u64]),
             "drtopk_server_drain": (st, [vp, i32]),
             "drtopk_server_usage": (st, [vp, P(sz), P(ctypes.c_int), P(ctypes.c_int)]),
+            "drtopk_server_stats": (st, [vp, P(ServerStats)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -157,10 +166,12 @@ def exported_symbols() -> list[str]:
 
 # ----------------------------------------------------------------- params
 def params(nbits: int = 8, alpha: int = -1, beta: int = 2, path: int = 0, algo="radix", num_bucket: int = 256,
-           largest: bool = True, sorted: bool = False, first_digits: int = 0) -> Params:
+           largest: bool = True, sorted: bool = False, first_digits: int = 0, team: int = 0) -> Params:
+    """team: 0 auto, 1 whole-GPU cooperative grid, 2 one thread-block cluster,
+    3 one CTA with the sets in shared memory, for the phases after the sampler."""
     p = Params()
     lib().drtopk_params_default(ctypes.byref(p))
-    p.nbits, p.alpha, p.beta, p.path = nbits, alpha, beta, path
+    p.nbits, p.alpha, p.beta, p.path, p.team = nbits, alpha, beta, path, team
     p.algo = _ALGOS[algo] if isinstance(algo, str) else int(algo)
     p.num_bucket, p.largest, p.sorted, p.first_digits = num_bucket, int(bool(largest)), int(bool(sorted)), first_digits
     return p
@@ -501,3 +512,9 @@ class Server:
         b, i, q = ctypes.c_size_t(0), ctypes.c_int(0), ctypes.c_int(0)
         check(lib().drtopk_server_usage(self._s, ctypes.byref(b), ctypes.byref(i), ctypes.byref(q)), "usage")
         return b.value, i.value, q.value
+
+    def stats(self) -> dict:
+        """Worker counters since creation (drtopk_server_stats)."""
+        st = ServerStats()
+        check(lib().drtopk_server_stats(self._s, ctypes.byref(st)), "drtopk_server_stats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}

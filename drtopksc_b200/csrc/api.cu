@@ -18,6 +18,7 @@
 #include "bitonic.cuh"
 #include "fused.cuh"
 #include "plan.h"
+#include "tail.cuh"
 #include "sampler.cuh"
 
 using namespace drtopk;
@@ -64,6 +65,106 @@ static void* fused_ptr(int km) {
     case KM_U32_MIN: return fused_fn<KM_U32_MIN>();
     default: return fused_fn<KM_F32_MIN>();
   }
+}
+
+template <int KM>
+static void* fused_cl_fn() {
+  return (void*)k_fused_cl<KM>;
+}
+static void* fused_cl_ptr(int km) {
+  switch (km) {
+    case KM_U32: return fused_cl_fn<KM_U32>();
+    case KM_F32: return fused_cl_fn<KM_F32>();
+    case KM_U32_MIN: return fused_cl_fn<KM_U32_MIN>();
+    default: return fused_cl_fn<KM_F32_MIN>();
+  }
+}
+
+// Largest cluster (16, else 8, else 4) of k_fused_cl CTAs that the device
+// can co-schedule with the largest dynamic shared memory a plan uses
+// (FUSED_CL_SMEM_MAX, set once as the kernel's limit); 0 if none.
+constexpr size_t FUSED_CL_SMEM_MAX = 100 * 1024;
+static int cluster_size(DevInfo* d, int km, size_t smem) {
+  static int cache[64][4];
+  if (smem > FUSED_CL_SMEM_MAX) return 0;
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  int& c = cache[d->device][km];
+  if (c != 0) return c > 0 ? c : 0;
+  void* fn = fused_cl_ptr(km);
+  c = -1;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FUSED_CL_SMEM_MAX) != cudaSuccess ||
+      cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  for (int want : {16, 8, 4}) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(want);
+    cfg.blockDim = dim3(FUSED_THREADS);
+    cfg.dynamicSmemBytes = FUSED_CL_SMEM_MAX;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = want;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, fn, &cfg) == cudaSuccess && ncl > 0) {
+      c = want;
+      break;
+    }
+    cudaGetLastError();
+  }
+  return c > 0 ? c : 0;
+}
+
+template <int KM>
+static void* tail_fn() {
+  return (void*)k_tail<KM>;
+}
+static void* tail_ptr(int km) {
+  switch (km) {
+    case KM_U32: return tail_fn<KM_U32>();
+    case KM_F32: return tail_fn<KM_F32>();
+    case KM_U32_MIN: return tail_fn<KM_U32_MIN>();
+    default: return tail_fn<KM_F32_MIN>();
+  }
+}
+static cudaLaunchConfig_t tail_config(cudaStream_t st, cudaLaunchAttribute* at) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(TAIL_CLUSTER);
+  cfg.blockDim = dim3(TAIL_THREADS);
+  cfg.dynamicSmemBytes = TAIL_SMEM;
+  cfg.stream = st;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = TAIL_CLUSTER;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+// whether the shared-memory tail cluster can run on this device (its
+// shared-memory limit is set once per device and key mode)
+static bool tail_ready(int device, int km) {
+  static int state[64][4];  // 0 unknown, 1 ready, -1 unavailable
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  if (device < 0 || device >= 64) return false;
+  int& s = state[device][km];
+  if (s == 0) {
+    s = -1;
+    cudaLaunchAttribute at[1];
+    cudaLaunchConfig_t cfg = tail_config(nullptr, at);
+    int ncl = 0;
+    if (cudaFuncSetAttribute(tail_ptr(km), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM) ==
+            cudaSuccess &&
+        cudaOccupancyMaxActiveClusters(&ncl, tail_ptr(km), &cfg) == cudaSuccess && ncl > 0)
+      s = 1;
+    else
+      cudaGetLastError();
+  }
+  return s > 0;
 }
 
 template <int KM>
@@ -325,6 +426,7 @@ struct drtopk_handle {
 };
 
 extern "C" void drtopk_params_default(drtopk_params_t* p) {
+  p->team = 0;
   p->nbits = 8;
   p->alpha = -1;
   p->beta = 2;
@@ -424,6 +526,44 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
                      split_grid(di, P->km, false, hs, &P->split_grid) != cudaSuccess))
       return DRTOPK_ECUDA;
   }
+  // team of the phases after the sampler: one CTA with the sets in shared
+  // memory when they are small (their cost is then round trips, not
+  // bandwidth), else the whole GPU; a thread-block cluster on request
+  P->cluster = 0;
+  P->tail = 0;
+  if (P->path != PATH_BITONIC) {
+    const int team = p ? p->team : 0;
+    const double dn = (double)n, dk = (double)k, S = (double)P->S;
+    // delegates, kept list and candidates must fit TAIL_CAP entries, and the
+    // concatenation must be short enough for one CTA to stream
+    const uint64_t Md = P->path == PATH_DEFAULT ? P->M : (P->path == PATH_BETA ? 2 * P->M : n);
+    const bool fits = !P->bucket && P->nb <= 256 && Md <= (uint64_t)TAIL_CAP && k <= (uint64_t)TAIL_CAP &&
+                      (!P->sorted || k <= (uint64_t)SMALL_SORT);
+    double gather = 0.0, cand = 0.0;
+    if (P->path == PATH_DEFAULT) {
+      gather = dk * S;
+      cand = dk;
+    } else if (P->path == PATH_BETA) {
+      const double q = dk / dn + std::ldexp(1.0, -8 * std::max(1, P->first_levels));
+      const double lam = q * S, e = std::exp(-lam), M = dn / S;
+      const double p_sel = 1.0 - e * (1.0 + lam);
+      gather = M * p_sel * S;
+      cand = M * lam * e + M * p_sel * (lam + 1.0);
+    } else {
+      cand = dn;
+    }
+    if (team == 3) {
+      if (!fits || !tail_ready(di->device, P->km)) return DRTOPK_EUNSUPPORTED;
+      P->tail = 1;
+    } else if (team == 0 && fits && gather <= TAIL_GATHER_AUTO && cand <= TAIL_CAP / 2 &&
+               tail_ready(di->device, P->km)) {
+      P->tail = 1;
+    } else if (team == 2) {
+      P->cluster = cluster_size(di, P->km, smem);
+      if (P->cluster <= 0) return DRTOPK_EUNSUPPORTED;
+    }
+    if (P->tail || P->cluster) P->split = 0;
+  }
   // sampler grid: persistent, capped by the work items
   if (P->path != PATH_PLAIN && !(P->path == PATH_BITONIC && P->normal)) {
     uint64_t items = P->alpha >= 9 ? P->M : ((n + 511) >> 9);
@@ -519,6 +659,24 @@ static drtopk_status_t launch_coop(void* fn, const Plan& P, void* argp, cudaStre
   return cudaLaunchKernelExC(&cfg, fn, args) == cudaSuccess ? DRTOPK_OK : DRTOPK_ECUDA;
 }
 
+static drtopk_status_t launch_cluster(const Plan& P, const FusedArgs* a, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(P.cluster);
+  cfg.blockDim = dim3(FUSED_THREADS);
+  cfg.dynamicSmemBytes = P.fused_smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = P.cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const FusedArgs* list = nullptr;
+  void* args[] = {const_cast<FusedArgs*>(a), &list};
+  return cudaLaunchKernelExC(&cfg, fused_cl_ptr(P.km), args) == cudaSuccess ? DRTOPK_OK : DRTOPK_ECUDA;
+}
+
 static drtopk_status_t enqueue_bitonic(const Plan& P, const void* d_keys, void* d_kth, void* d_vals, int64_t* d_idx,
                                        char* ws, cudaStream_t st, cudaEvent_t* ev) {
   char* ctrl = ws + P.off_ctrl;
@@ -544,7 +702,6 @@ static drtopk_status_t enqueue_bitonic(const Plan& P, const void* d_keys, void* 
   b.out_idx = d_idx;
   b.stats = cw + CW_STATS;
   b.gb.count = cw + CW_BAR_COUNT;
-  b.gb.gen = cw + CW_BAR_GEN;
   b.gb.err = cw + CW_ERR;
   b.gb.nblocks = (uint32_t)P.fused_grid;
   if (!P.normal) {
@@ -598,10 +755,10 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
   a.stats = cw + CW_STATS;
   a.sort_tot = cw + CTRL_HDR_WORDS + 4 * (size_t)P.run_words;
   a.gb.count = cw + CW_BAR_COUNT;
-  a.gb.gen = cw + CW_BAR_GEN;
   a.gb.err = cw + CW_ERR;
   a.gb.nblocks = (uint32_t)P.fused_grid;
   a.thr_word = cw + CW_THR;
+  a.tail_flag = cw + CW_TAIL;
   a.phase_lo = 1;
   a.phase_hi = 3;
   a.out_kth = static_cast<uint32_t*>(d_kth);
@@ -648,7 +805,16 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
   if (ev) cudaEventRecord(ev[1], st);
   // ---- fused cooperative kernel (split mode: phase 1, concatenation kernels, phase 3)
   drtopk_status_t s;
-  if (!P.split) {
+  if (P.tail) {
+    a.gb.nblocks = TAIL_CLUSTER;
+    cudaLaunchAttribute at[1];
+    cudaLaunchConfig_t cfg = tail_config(st, at);
+    void* args[] = {&a};
+    s = cudaLaunchKernelExC(&cfg, tail_ptr(P.km), args) == cudaSuccess ? DRTOPK_OK : DRTOPK_ECUDA;
+  } else if (P.cluster > 0) {
+    a.gb.nblocks = (uint32_t)P.cluster;
+    s = launch_cluster(P, &a, st);
+  } else if (!P.split) {
     s = launch_coop(fused_ptr(P.km), P, &a, st);
   } else {
     a.phase_hi = 1;
@@ -799,6 +965,8 @@ extern "C" drtopk_status_t drtopk_last_stats(drtopk_handle_t h, drtopk_stats_t* 
     st->ms_concat = t2 > t1 ? (t2 - t1) * 1e-6 : 0.0;
     st->ms_second = t3 > t2 ? (t3 - t2) * 1e-6 : 0.0;
     st->ms_total = ms_all;
+    st->team_ctas = P.tail ? TAIL_CLUSTER : (P.cluster > 0 ? P.cluster : P.fused_grid);
+    st->team_cluster = P.tail ? 3 : (P.cluster > 0 ? 1 : 0);
   }
   cudaSetDevice(cur);
   return s;
@@ -880,7 +1048,6 @@ static double cost_beta(double n, double k, double S, int digits) {
 
 extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_t dtype, drtopk_params_t* p) {
   if (!p || n == 0 || k < 1 || k > n) return DRTOPK_EINVAL;
-  (void)dtype;
   if (p->algo == DRTOPK_ALGO_AUTO) p->algo = DRTOPK_ALGO_RADIX;
   if (p->algo == DRTOPK_ALGO_BITONIC) {
     if (p->alpha < 0) {
@@ -908,8 +1075,11 @@ extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_
       if (c < best) { best = c; best_alpha = alpha; best_path = 1; best_digits = 0; }
     }
     if (2 * M >= k && p->beta == 2) {
+      // float keys crowd into a few top bytes (sign and exponent): a one-digit
+      // threshold would admit far more candidates than the model says
       const int maxd = p->nbits == 8 ? 2 : 1;
-      for (int d = 1; d <= maxd; ++d) {
+      const int mind = (p->nbits == 8 && dtype == DRTOPK_F32) ? 2 : 1;
+      for (int d = mind; d <= maxd; ++d) {
         const double c = cost_beta(dn, dk, S, p->nbits == 8 ? d : (32 / p->nbits - 3));
         if (c < best) { best = c; best_alpha = alpha; best_path = 2; best_digits = d; }
       }
@@ -1088,7 +1258,6 @@ extern "C" drtopk_status_t drtopk_selftest_wait_timeout(int device, double* ms_w
   if (s == DRTOPK_OK) {
     GridBar gb;
     gb.count = w;
-    gb.gen = w + 1;
     gb.err = w + 2;
     gb.nblocks = 2;           // one CTA more than launched: nothing completes the barrier
     gb.spin_limit = 1u << 22; // ~0.5 s of polls

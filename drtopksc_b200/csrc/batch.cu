@@ -106,7 +106,6 @@ drtopk_status_t enqueue_batch(drtopk_batch* b, const void* d_keys, void* d_kth, 
   a.out_kth = static_cast<uint32_t*>(d_kth);
   a.out_vals = static_cast<uint32_t*>(d_vals);
   a.out_idx = d_idx;
-  a.sorted = b->sorted;
   return launch_segmented(a, b->grid, b->smem, st) == cudaSuccess ? DRTOPK_OK : DRTOPK_ECUDA;
 }
 
@@ -154,6 +153,7 @@ extern "C" drtopk_status_t drtopk_batch_plan(drtopk_batch_t b, int nseg, const u
     d.key_off = h_offsets[s];
     d.len = (uint32_t)len;
     d.k = k;
+    d.sorted = sorted;
     d.km = dt == DRTOPK_F32 ? KM_F32 : KM_U32;
     choose(d.len, k, d.mode, d.alpha);
     d.out_off = out_total;

@@ -126,6 +126,21 @@ DRTOPK_DEV uint32_t warp_append(bool pred, uint32_t* counter) {
   return base + __popc(b & ((1u << lane) - 1u));
 }
 
+// Histogram increment with a fast path for warps whose active lanes all hit
+// one bin (one shared-memory atomic for the warp): skewed sets -- delegates
+// are subrange maxima and crowd into the top bins -- would otherwise
+// serialise 32 atomics on one address.  Mixed warps add per lane.
+DRTOPK_DEV void hist_add_warp(uint32_t* h, uint32_t bin) {
+  const unsigned mask = __activemask();
+  const int leader = __ffs(mask) - 1;
+  const uint32_t b0 = __shfl_sync(mask, bin, leader);
+  if (__all_sync(mask, bin == b0)) {
+    if ((int)lane_id() == leader) atomicAdd(&h[bin], (uint32_t)__popc(mask));
+  } else {
+    atomicAdd(&h[bin], 1u);
+  }
+}
+
 // Block-aggregated append to two lists: every thread of the block passes the
 // number of items it will write to list A and list B (each < 2^16 summed
 // over the block); one atomic per list per call; returns this thread's
@@ -200,6 +215,27 @@ DRTOPK_DEV uint32_t block_append1(uint32_t c, uint32_t* counter) {
   return r;
 }
 
+// Block-strided loop over [0, n) that issues U loads per thread before
+// using any of them: ld(i) for every index of a round, then use(i, value).
+// A plain strided loop waits one memory round trip per iteration.
+template <int U, typename LD, typename USE>
+DRTOPK_DEV void block_load_loop(uint32_t n, LD&& ld, USE&& use) {
+  using V = decltype(ld(0u));
+  for (uint32_t b = 0; b < n; b += blockDim.x * U) {
+    V v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint32_t i = b + u * blockDim.x + threadIdx.x;
+      if (i < n) v[u] = ld(i);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint32_t i = b + u * blockDim.x + threadIdx.x;
+      if (i < n) use(i, v[u]);
+    }
+  }
+}
+
 // ------------------------------------------------------------------ errors
 enum DevErr : uint32_t {
   DE_BARRIER_TIMEOUT = 1u,   // a grid barrier gave up waiting
@@ -208,49 +244,115 @@ enum DevErr : uint32_t {
 };
 
 // Grid barrier for kernels launched cooperatively (all CTAs co-resident).
-// The spin is bounded: after ~2^26 polls (~seconds) the CTA records
-// DE_BARRIER_TIMEOUT and every later barrier returns false immediately, so a
-// broken launch ends with an error instead of a hang.
+// One 32-bit word holds (generation << 16) | arrivals: a CTA arrives with one
+// acq_rel atomic; the last arrival resets the count and opens the next
+// generation with a second atomic, and the others poll the word for the
+// generation change.  The spin is bounded: after ~2^26 polls (~seconds) the
+// CTA records DE_BARRIER_TIMEOUT; a CTA that finds the flag set while it
+// waits returns false at once, so a broken launch ends with an error
+// instead of a hang.
 struct GridBar {
-  uint32_t* count;   // arrivals in the current generation
-  uint32_t* gen;     // generation number
+  uint32_t* count;   // (generation << 16) | arrivals in this generation
   uint32_t* err;     // error word (host-visible)
-  uint32_t nblocks;
+  uint32_t nblocks;  // < 2^16
   uint32_t spin_limit;  // polls before giving up (0: default 2^26)
 };
+
+DRTOPK_DEV uint32_t atom_add_acq_rel_gpu(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+DRTOPK_DEV void red_add_release_gpu(uint32_t* p, uint32_t v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 DRTOPK_DEV bool grid_barrier(const GridBar& gb) {
   __shared__ uint32_t s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t ok = 1;
-    if (ld_acquire_gpu(gb.err) & DE_BARRIER_TIMEOUT) ok = 0;
-    if (ok) {
-      uint32_t g = ld_acquire_gpu(gb.gen);
-      __threadfence();
-      uint32_t arrived = atomicAdd(gb.count, 1u);
-      if (arrived == gb.nblocks - 1) {
-        atomicExch(gb.count, 0u);
-        __threadfence();
-        st_release_gpu(gb.gen, g + 1);
-      } else {
-        uint32_t it = 0;
-        const uint32_t lim = gb.spin_limit ? gb.spin_limit : (1u << 26);
-        while (ld_acquire_gpu(gb.gen) == g) {
-          if (++it > lim) {
-            atomicOr(gb.err, (uint32_t)DE_BARRIER_TIMEOUT);
-            ok = 0;
-            break;
-          }
-          if ((it & 1023u) == 0 && (ld_acquire_gpu(gb.err) & DE_BARRIER_TIMEOUT)) { ok = 0; break; }
-          __nanosleep(64);
+    const uint32_t old = atom_add_acq_rel_gpu(gb.count, 1u);
+    if ((old & 0xffffu) == gb.nblocks - 1) {
+      red_add_release_gpu(gb.count, 0x10000u - gb.nblocks);
+    } else {
+      const uint32_t g = old >> 16;
+      const uint32_t lim = gb.spin_limit ? gb.spin_limit : (1u << 26);
+      uint32_t it = 0;
+      while ((ld_acquire_gpu(gb.count) >> 16) == g) {
+        if (++it > lim) {
+          atomicOr(gb.err, (uint32_t)DE_BARRIER_TIMEOUT);
+          ok = 0;
+          break;
         }
+        if ((it & 1023u) == 1u && (ld_acquire_gpu(gb.err) & DE_BARRIER_TIMEOUT)) { ok = 0; break; }
+        __nanosleep(32);
       }
     }
     s_ok = ok;
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+// A team of CTAs working on one problem: the whole grid of a cooperative
+// launch (software grid barrier above), one thread-block cluster (hardware
+// cluster barrier, ~0.2 us) or a single CTA.  Code written against a Team
+// distributes work by (rank, size) and synchronises with team_sync; every
+// CTA of a team must reach the same team_sync calls (control flow that
+// leads to a team_sync depends only on kernel arguments and on values read
+// after the previous team_sync).
+struct Team {
+  GridBar gb;     // grid teams: barrier words
+  uint32_t rank;  // this CTA's index in the team
+  uint32_t size;  // CTAs in the team
+  int cluster;    // 0: grid team; 1: this CTA's thread-block cluster; 2: this CTA alone
+};
+
+DRTOPK_DEV uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+DRTOPK_DEV uint32_t cluster_nctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+DRTOPK_DEV uint32_t cluster_id_x() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+  return r;
+}
+
+DRTOPK_DEV Team grid_team(const GridBar& gb) {
+  Team t;
+  t.gb = gb;
+  t.rank = blockIdx.x;
+  t.size = gridDim.x;
+  t.cluster = 0;
+  return t;
+}
+DRTOPK_DEV Team cluster_team() {
+  Team t = {};
+  t.rank = cluster_ctarank();
+  t.size = cluster_nctarank();
+  t.cluster = 1;
+  return t;
+}
+
+DRTOPK_DEV bool team_sync(const Team& t) {
+  if (t.cluster == 2) {
+    __syncthreads();  // one CTA: a block barrier orders its global-memory accesses
+    return true;
+  }
+  if (t.cluster == 1) {
+    // all threads of every CTA in the cluster arrive; release/acquire at
+    // cluster scope orders the global-memory writes made before it
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+    return true;
+  }
+  return grid_barrier(t.gb);
 }
 
 }  // namespace drtopk

@@ -16,9 +16,10 @@
 // w = (hi-lo)/nb + 1 over a [min,max] range (exact restatement of
 // bucket_select/bucketselect_combined.cuh).
 //
-// All CTAs of the (cooperative) kernel execute the same sequence; the pick
-// is recomputed redundantly in every CTA from the global histogram, so the
-// replicated level state stays identical without extra broadcasts.
+// All CTAs of a team (the grid of a cooperative kernel, one thread-block
+// cluster, or one CTA) execute the same sequence; the pick is recomputed
+// redundantly in every CTA from the global histogram, so the replicated
+// level state stays identical without extra broadcasts.
 #pragma once
 
 #include "common.cuh"
@@ -26,6 +27,7 @@
 namespace drtopk {
 
 constexpr int FUSED_THREADS = 256;
+constexpr int MAX_BLOCK_WARPS = 16;  // CTAs of up to 512 threads (the shared-memory tail uses 512)
 constexpr int MAX_LEVELS = 40;
 
 constexpr int SMALL_SET = 4096;  // a set this small is finished by one CTA in shared memory
@@ -87,11 +89,12 @@ struct Pick {
 // H in global memory (written by other CTAs) or, with SMEM, shared memory.
 template <bool SMEM = false>
 DRTOPK_DEV Pick block_pick(const uint32_t* H, int nb, uint32_t R) {
-  __shared__ uint32_t s_part[FUSED_THREADS / 32];
+  __shared__ uint32_t s_part[32];
   __shared__ Pick s_pick;
   __shared__ int s_found;
   const int t = threadIdx.x;
-  const int q = (nb + FUSED_THREADS - 1) / FUSED_THREADS;
+  const int nthr = blockDim.x;
+  const int q = (nb + nthr - 1) / nthr;
   const int b0 = min(nb, t * q), b1 = min(nb, b0 + q);
   auto hb = [&](int b) { return SMEM ? H[b] : ld_cg_u32(H + b); };
   uint32_t local = 0;
@@ -108,7 +111,7 @@ DRTOPK_DEV Pick block_pick(const uint32_t* H, int nb, uint32_t R) {
   if (t == 0) s_found = 0;
   __syncthreads();
   uint32_t wbase = 0, total = 0;
-  for (int w = 0; w < FUSED_THREADS / 32; ++w) {
+  for (int w = 0; w < nthr / 32; ++w) {
     if (w < (t >> 5)) wbase += s_part[w];
     total += s_part[w];
   }
@@ -156,9 +159,9 @@ DRTOPK_DEV bool advance(const EngineCfg& c, const Level& L, const Pick& p, int l
 }
 
 // --------------------------------------------------------------- helpers
-DRTOPK_DEV void zero_words(uint32_t* p, int n) {
-  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+DRTOPK_DEV void zero_words(const Team& tm, uint32_t* p, int n) {
+  const uint64_t g = (uint64_t)tm.rank * blockDim.x + threadIdx.x;
+  const uint64_t G = (uint64_t)tm.size * blockDim.x;
   for (uint64_t i = g; i < (uint64_t)n; i += G) p[i] = 0;
 }
 
@@ -187,10 +190,10 @@ DRTOPK_DEV uint32_t src_key1(const Src& s, uint64_t i) {
 // per block.  fn(key, payload, valid) is called for every slot; valid=false
 // for padding.  Used by histogram passes (no appends inside fn).
 template <int KM, typename F>
-DRTOPK_DEV void for_each_src(const Src& s, bool from_pairs, uint64_t count, F&& fn) {
+DRTOPK_DEV void for_each_src(const Team& tm, const Src& s, bool from_pairs, uint64_t count, F&& fn) {
   constexpr int E = 16;
   const uint64_t T = (uint64_t)blockDim.x * E;
-  for (uint64_t tb = (uint64_t)blockIdx.x * T; tb < count; tb += (uint64_t)gridDim.x * T) {
+  for (uint64_t tb = (uint64_t)tm.rank * T; tb < count; tb += (uint64_t)tm.size * T) {
     uint32_t key[E], pay[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -219,11 +222,11 @@ constexpr int SPLIT_E = 16;  // entries per thread per tile
 // -> next set (+ histogram of the next level).  Tiles of blockDim*SPLIT_E
 // entries, coalesced loads, one block-aggregated append per tile.
 template <int KM>
-DRTOPK_DEV void split_tiles(const EngineCfg& c, const Src& s, bool pairs, uint64_t count, const Level& N,
-                            bool want_hist, uint2* top, uint32_t* top_count, uint2* nxt, uint32_t* nxt_count,
-                            uint32_t* s_hist) {
+DRTOPK_DEV void split_tiles(const Team& tm, const EngineCfg& c, const Src& s, bool pairs, uint64_t count,
+                            const Level& N, bool want_hist, uint2* top, uint32_t* top_count, uint2* nxt,
+                            uint32_t* nxt_count, uint32_t* s_hist) {
   const uint64_t T = (uint64_t)blockDim.x * SPLIT_E;
-  for (uint64_t tb = (uint64_t)blockIdx.x * T; tb < count; tb += (uint64_t)gridDim.x * T) {
+  for (uint64_t tb = (uint64_t)tm.rank * T; tb < count; tb += (uint64_t)tm.size * T) {
     uint32_t val[SPLIT_E], pay[SPLIT_E];
     uint32_t up = 0, in = 0, ca = 0, cb = 0;
 #pragma unroll
@@ -259,7 +262,7 @@ DRTOPK_DEV void split_tiles(const EngineCfg& c, const Src& s, bool pairs, uint64
       if ((in >> e) & 1u) {
         nxt[sl.b++] = make_uint2(val[e], pay[e]);
         const uint32_t key = c.key_from_payload ? ~pay[e] : val[e];
-        if (want_hist) atomicAdd(&s_hist[bin_of(key, N.lo, N.w, N.wshift)], 1u);
+        if (want_hist) hist_add_warp(s_hist, bin_of(key, N.lo, N.w, N.wshift));
       }
     }
   }
@@ -273,7 +276,7 @@ DRTOPK_DEV void split_tiles(const EngineCfg& c, const Src& s, bool pairs, uint64
 // Returns the level index that finished and the final Level through Lout.
 template <int KM>
 DRTOPK_DEV int run_levels(const EngineCfg& c, const Src& src0, bool src0_pairs, const RunBufs& rb, Level L,
-                          uint32_t* s_hist, const GridBar& gb, Level& Lout, Pick& last_pick, int& eq_buf,
+                          uint32_t* s_hist, const Team& tm, Level& Lout, Pick& last_pick, int& eq_buf,
                           uint64_t& eq_count, bool& ok, bool small_exit = false, bool* went_small = nullptr) {
   int j = 0;
   ok = true;
@@ -284,7 +287,7 @@ DRTOPK_DEV int run_levels(const EngineCfg& c, const Src& src0, bool src0_pairs, 
     Level N;
     bool done = advance(c, L, p, j, N);
     last_pick = p;
-    zero_words(rb.H[(j + 2) % 3], c.nb);
+    zero_words(tm, rb.H[(j + 2) % 3], c.nb);
     uint32_t* Hn = rb.H[(j + 1) % 3];
     const bool want_hist = !done;
     clear_hist(s_hist, c.nb);
@@ -292,11 +295,11 @@ DRTOPK_DEV int run_levels(const EngineCfg& c, const Src& src0, bool src0_pairs, 
       if (done) { Lout = N; break; }
       // histogram the members of the new range over the level-0 source
       const uint64_t cnt = src0_pairs ? (uint64_t)ld_cg_u32(src0.count_dev) : src0.count;
-      for_each_src<KM>(src0, src0_pairs, cnt, [&](uint32_t key, uint32_t, bool valid) {
-        if (valid && key >= N.lo && key <= N.hi) atomicAdd(&s_hist[bin_of(key, N.lo, N.w, N.wshift)], 1u);
+      for_each_src<KM>(tm, src0, src0_pairs, cnt, [&](uint32_t key, uint32_t, bool valid) {
+        if (valid && key >= N.lo && key <= N.hi) hist_add_warp(s_hist, bin_of(key, N.lo, N.w, N.wshift));
       });
       flush_hist(s_hist, Hn, c.nb);
-      if (!grid_barrier(gb)) { ok = false; break; }
+      if (!team_sync(tm)) { ok = false; break; }
       L = N;
       continue;
     }
@@ -310,10 +313,10 @@ DRTOPK_DEV int run_levels(const EngineCfg& c, const Src& src0, bool src0_pairs, 
       s.pairs = rb.cbuf[(j - 1) & 1];
       cnt = ld_cg_u32(rb.set_count + j);
     }
-    split_tiles<KM>(c, s, from_pairs, cnt, N, want_hist, rb.top, rb.top_count, rb.cbuf[j & 1], rb.set_count + j + 1,
-                    s_hist);
+    split_tiles<KM>(tm, c, s, from_pairs, cnt, N, want_hist, rb.top, rb.top_count, rb.cbuf[j & 1],
+                    rb.set_count + j + 1, s_hist);
     if (want_hist) flush_hist(s_hist, Hn, c.nb);
-    if (!grid_barrier(gb)) { ok = false; break; }
+    if (!team_sync(tm)) { ok = false; break; }
     L = N;
     if (done) {
       Lout = N;
@@ -349,6 +352,169 @@ DRTOPK_DEV void block_bitonic_asc(uint64_t* s, int npow2) {
   __syncthreads();
 }
 
+// histogram of the bins of sA[0..n) in shared memory (one CTA), four
+// independent entries per thread per round
+DRTOPK_DEV void smem_hist(const uint2* sA, uint32_t n, const Level& L, uint32_t* s_hist) {
+  for (uint32_t i0 = threadIdx.x; i0 < n; i0 += 4 * blockDim.x) {
+    uint32_t b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t i = i0 + u * blockDim.x;
+      b[u] = i < n ? bin_of(sA[i].x, L.lo, L.w, L.wshift) : 0xffffffffu;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (b[u] != 0xffffffffu) hist_add_warp(s_hist, b[u]);
+  }
+}
+
+// The pick rule of block_pick, by one warp scanning a shared-memory
+// histogram (nb <= 4096): lane l owns bins [l*per, (l+1)*per); one block
+// barrier publishes the result.
+DRTOPK_DEV Pick warp_pick_smem(const uint32_t* H, int nb, uint32_t R) {
+  __shared__ Pick s_wpick;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    const int per = (nb + 31) / 32;
+    const int b0 = min(nb, lane * per), b1 = min(nb, b0 + per);
+    uint32_t local = 0;
+    for (int b = b0; b < b1; ++b) local += H[b];
+    // suffix sum over lanes: bins at and above this lane's
+    uint32_t suf = local;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_down_sync(0xffffffffu, suf, off);
+      if (lane + off < 32) suf += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, suf, 0);
+    const uint32_t above = suf - local;
+    const bool mine = local > 0 && above < R && R <= above + local;
+    if (mine) {
+      uint32_t acc = above;
+      for (int b = b1 - 1; b >= b0; --b) {
+        const uint32_t c = H[b];
+        if (acc + c >= R) {
+          s_wpick.b = b;
+          s_wpick.cnt = c;
+          s_wpick.above = acc;
+          break;
+        }
+        acc += c;
+      }
+    }
+    if (__ballot_sync(0xffffffffu, mine) == 0u && lane == 0) {
+      // R exceeds the set: the reference's rule then picks bin 0
+      s_wpick.b = 0;
+      s_wpick.cnt = H[0];
+      s_wpick.above = total - H[0];
+    }
+  }
+  __syncthreads();
+  const Pick p = s_wpick;
+  return p;
+}
+
+// min and max key of sA[0..n) (one CTA); ends with a block barrier
+DRTOPK_DEV void block_minmax(const uint2* sA, uint32_t n, uint32_t& mn, uint32_t& mx) {
+  __shared__ uint32_t s_mn[32], s_mx[32];
+  uint32_t a = 0xffffffffu, b = 0u;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t k = sA[i].x;
+    a = min(a, k);
+    b = max(b, k);
+  }
+  a = __reduce_min_sync(0xffffffffu, a);
+  b = __reduce_max_sync(0xffffffffu, b);
+  if ((threadIdx.x & 31u) == 0) {
+    s_mn[threadIdx.x >> 5] = a;
+    s_mx[threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  mn = 0xffffffffu;
+  mx = 0u;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    mn = min(mn, s_mn[w]);
+    mx = max(mx, s_mx[w]);
+  }
+  __syncthreads();  // s_mn / s_mx may be rewritten by the next call
+}
+
+// Pick of one level over sA[0..n) in shared memory (one CTA): when the
+// whole set lies in one bin (common for delegates, which crowd into the top
+// bins) its min and max show it without a histogram; else histogram + pick.
+DRTOPK_DEV Pick smem_level_pick(const uint2* sA, uint32_t n, const Level& L, int nb, uint32_t* s_hist) {
+  uint32_t mn, mx;
+  block_minmax(sA, n, mn, mx);
+  if (n > 0 && L.R <= n && mn >= L.lo && mx <= L.hi &&
+      bin_of(mn, L.lo, L.w, L.wshift) == bin_of(mx, L.lo, L.w, L.wshift)) {
+    Pick p;
+    p.b = bin_of(mn, L.lo, L.w, L.wshift);
+    p.cnt = n;
+    p.above = 0;
+    return p;
+  }
+  clear_hist(s_hist, nb);
+  smem_hist(sA, n, L, s_hist);
+  __syncthreads();
+  return warp_pick_smem(s_hist, nb, L.R);
+}
+
+// Stable two-way split of src[0..n) by one CTA: entries with key > hi (when
+// want_a) are appended to outA at *cntA, entries with lo <= key <= hi to
+// outB at *cntB (counters in shared or global memory, advanced by one atomic
+// each).  Every warp owns a contiguous segment of the input and writes
+// contiguous runs ranked by ballots: no shared-memory bank conflicts, index
+// order kept.  Ends with a block barrier.
+DRTOPK_DEV void split_block(const uint2* src, uint32_t n, uint32_t lo, uint32_t hi, bool want_a, uint2* outA,
+                            uint32_t* cntA, uint2* outB, uint32_t* cntB) {
+  __shared__ uint32_t s_wa[32], s_wb[32], s_base[2];
+  const unsigned lane = threadIdx.x & 31u;
+  const int w = threadIdx.x >> 5, W = blockDim.x >> 5;
+  const uint32_t per = (((n + W - 1) / W) + 31u) & ~31u;
+  const uint32_t b0 = min(n, (uint32_t)w * per), b1 = min(n, b0 + per);
+  uint32_t ca = 0, cb = 0;
+  for (uint32_t c = b0; c < b1; c += 32) {
+    const uint32_t i = c + lane;
+    const bool v = i < b1;
+    const uint32_t key = v ? src[i].x : 0u;
+    ca += __popc(__ballot_sync(0xffffffffu, v && want_a && key > hi));
+    cb += __popc(__ballot_sync(0xffffffffu, v && key >= lo && key <= hi));
+  }
+  if (lane == 0) {
+    s_wa[w] = ca;
+    s_wb[w] = cb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t ta = 0, tb = 0;
+    for (int q = 0; q < W; ++q) {
+      const uint32_t xa = s_wa[q], xb = s_wb[q];
+      s_wa[q] = ta;
+      s_wb[q] = tb;
+      ta += xa;
+      tb += xb;
+    }
+    s_base[0] = ta ? atomicAdd(cntA, ta) : 0u;
+    s_base[1] = tb ? atomicAdd(cntB, tb) : 0u;
+  }
+  __syncthreads();
+  uint32_t pa = s_base[0] + s_wa[w], pb = s_base[1] + s_wb[w];
+  const unsigned lt = (1u << lane) - 1u;
+  for (uint32_t c = b0; c < b1; c += 32) {
+    const uint32_t i = c + lane;
+    const bool v = i < b1;
+    const uint2 e = v ? src[i] : make_uint2(0u, 0u);
+    const bool ia = v && want_a && e.x > hi;
+    const bool ib = v && e.x >= lo && e.x <= hi;
+    const unsigned ma = __ballot_sync(0xffffffffu, ia), mb = __ballot_sync(0xffffffffu, ib);
+    if (ia) outA[pa + __popc(ma & lt)] = e;
+    if (ib) outB[pb + __popc(mb & lt)] = e;
+    pa += __popc(ma);
+    pb += __popc(mb);
+  }
+  __syncthreads();
+}
+
 // Completion of a run inside ONE CTA once its remaining set (cnt <=
 // SMALL_SET entries) fits in shared memory: the same levels (pick /
 // advance / split), then the tie fill by lowest payload, with block
@@ -358,48 +524,38 @@ template <int KM>
 DRTOPK_DEV void block_finish(const EngineCfg& c, const Src& src, bool pairs, uint32_t cnt, Level L, int j,
                              const RunBufs& rb, uint32_t* s_hist, uint2* sA, uint2* sB) {
   __shared__ uint32_t s_n;
-  for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-    if (pairs) sA[i] = ld_cg_v2(reinterpret_cast<const uint32_t*>(src.pairs + i));
-    else sA[i] = make_uint2(src_key1<KM>(src, i), i);
-  }
+  if (pairs)
+    block_load_loop<8>(cnt, [&](uint32_t i) { return ld_cg_v2(reinterpret_cast<const uint32_t*>(src.pairs + i)); },
+                       [&](uint32_t i, uint2 v) { sA[i] = v; });
+  else
+    block_load_loop<8>(cnt, [&](uint32_t i) { return src_key1<KM>(src, i); },
+                       [&](uint32_t i, uint32_t v) { sA[i] = make_uint2(v, i); });
+  __syncthreads();
   uint32_t n = cnt;
   bool ok = true;
   for (;;) {
     if (j >= MAX_LEVELS) { ok = false; break; }
-    clear_hist(s_hist, c.nb);
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
-      atomicAdd(&s_hist[bin_of(sA[i].x, L.lo, L.w, L.wshift)], 1u);
-    __syncthreads();
-    const Pick p = block_pick<true>(s_hist, c.nb, L.R);
+    const Pick p = smem_level_pick(sA, n, L, c.nb, s_hist);
     Level N;
     const bool done = advance(c, L, p, j, N);
-    if (threadIdx.x == 0) s_n = 0;
-    __syncthreads();
-    for (uint32_t base = 0; base < n; base += blockDim.x) {
-      const uint32_t i = base + threadIdx.x;
-      const uint2 e = i < n ? sA[i] : make_uint2(0u, 0u);
-      const bool up = i < n && e.x > N.hi;
-      const bool in = i < n && e.x >= N.lo && e.x <= N.hi;
-      const uint32_t s1 = block_append1(up, rb.top_count);
-      if (up) rb.top[s1] = e;
-      const uint32_t s2 = block_append1(in, &s_n);
-      if (in) sB[s2] = e;
+    if (p.cnt != n) {  // else the whole set is in the chosen bin: nothing moves
+      if (threadIdx.x == 0) s_n = 0;
+      __syncthreads();
+      split_block(sA, n, N.lo, N.hi, true, rb.top, rb.top_count, sB, &s_n);
+      n = s_n;
+      uint2* t = sA; sA = sB; sB = t;
     }
-    __syncthreads();
-    n = s_n;
-    uint2* t = sA; sA = sB; sB = t;
     L = N;
     ++j;
     if (done) break;
   }
   const uint32_t R = L.R;
   const uint32_t kth = (n == 1) ? sA[0].x : L.lo;
+  __shared__ uint32_t s_tb;
   if (ok && n == R) {
-    for (uint32_t base = 0; base < n; base += blockDim.x) {
-      const uint32_t i = base + threadIdx.x;
-      const uint32_t s1 = block_append1(i < n, rb.top_count);
-      if (i < n) rb.top[s1] = sA[i];
-    }
+    if (threadIdx.x == 0) s_tb = atomicAdd(rb.top_count, n);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) rb.top[s_tb + i] = sA[i];
   } else if (ok && n > R) {
     // keep the R lowest payloads among the tied entries
     uint64_t* w = reinterpret_cast<uint64_t*>(sB);
@@ -408,11 +564,10 @@ DRTOPK_DEV void block_finish(const EngineCfg& c, const Src& src, bool pairs, uin
     for (int i = threadIdx.x; i < np2; i += blockDim.x)
       w[i] = i < (int)n ? (((uint64_t)sA[i].y << 32) | sA[i].x) : ~0ull;
     block_bitonic_asc(w, np2);
-    for (uint32_t base = 0; base < R; base += blockDim.x) {
-      const uint32_t i = base + threadIdx.x;
-      const uint32_t s1 = block_append1(i < R, rb.top_count);
-      if (i < R) rb.top[s1] = make_uint2((uint32_t)w[i], (uint32_t)(w[i] >> 32));
-    }
+    if (threadIdx.x == 0) s_tb = atomicAdd(rb.top_count, R);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < R; i += blockDim.x)
+      rb.top[s_tb + i] = make_uint2((uint32_t)w[i], (uint32_t)(w[i] >> 32));
   } else {
     ok = false;
   }
@@ -427,13 +582,13 @@ DRTOPK_DEV void block_finish(const EngineCfg& c, const Src& src, bool pairs, uin
 
 // histogram pass of level 0 for a run: hist of bin_of(key, L0) over the source
 template <int KM>
-DRTOPK_DEV void hist_pass(const Src& src, bool pairs, bool key_from_payload, const Level& L0, int nb, uint32_t* gH,
-                          uint32_t* s_hist) {
+DRTOPK_DEV void hist_pass(const Team& tm, const Src& src, bool pairs, bool key_from_payload, const Level& L0, int nb,
+                          uint32_t* gH, uint32_t* s_hist) {
   clear_hist(s_hist, nb);
   const uint64_t cnt = pairs ? (uint64_t)ld_cg_u32(src.count_dev) : src.count;
-  for_each_src<KM>(src, pairs, cnt, [&](uint32_t val, uint32_t pay, bool valid) {
+  for_each_src<KM>(tm, src, pairs, cnt, [&](uint32_t val, uint32_t pay, bool valid) {
     const uint32_t key = key_from_payload ? ~pay : val;
-    if (valid && key >= L0.lo && key <= L0.hi) atomicAdd(&s_hist[bin_of(key, L0.lo, L0.w, L0.wshift)], 1u);
+    if (valid && key >= L0.lo && key <= L0.hi) hist_add_warp(s_hist, bin_of(key, L0.lo, L0.w, L0.wshift));
   });
   flush_hist(s_hist, gH, nb);
 }
@@ -458,13 +613,13 @@ DRTOPK_DEV Level bucket_level0(uint32_t mn, uint32_t mx, int nb, uint32_t R) {
 // compact buffers alias rb's).
 template <int KM>
 DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_pairs, const RunBufs& rb,
-                                const RunBufs& fb, Level L0, uint32_t* s_hist, const GridBar& gb,
+                                const RunBufs& fb, Level L0, uint32_t* s_hist, const Team& tm,
                                 uint2* s_fast = nullptr) {
   RunResult res = {0u, 0u, 0, 1};
   const bool can_small = s_fast && !c.thr_only && !c.key_from_payload;
   auto finish_small = [&](const Src& s, bool pairs, uint32_t cnt, const Level& L, int j0) {
-    if (blockIdx.x == 0) block_finish<KM>(c, s, pairs, cnt, L, j0, rb, s_hist, s_fast, s_fast + SMALL_SET);
-    if (!grid_barrier(gb)) { res.ok = 0; return; }
+    if (tm.rank == 0) block_finish<KM>(c, s, pairs, cnt, L, j0, rb, s_hist, s_fast, s_fast + SMALL_SET);
+    if (!team_sync(tm)) { res.ok = 0; return; }
     res.thr = ld_cg_u32(rb.res);
     res.kth = ld_cg_u32(rb.res + 1);
     res.levels = (int)ld_cg_u32(rb.res + 2);
@@ -482,7 +637,7 @@ DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_p
   int eqb = 0;
   uint64_t E = 0;
   bool ok = true, small = false;
-  int j = run_levels<KM>(c, src0, src0_pairs, rb, L0, s_hist, gb, Lf, lp, eqb, E, ok, can_small, &small);
+  int j = run_levels<KM>(c, src0, src0_pairs, rb, L0, s_hist, tm, Lf, lp, eqb, E, ok, can_small, &small);
   res.levels = j + 1;
   res.thr = Lf.lo;
   if (!ok) { res.ok = 0; return res; }
@@ -499,12 +654,12 @@ DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_p
   if (E == R) {
     // every tied entry is kept: they go after the G = k0 - R entries above
     const uint64_t G0 = (uint64_t)ld_cg_u32(rb.top_count);
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t Gs = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t g = (uint64_t)tm.rank * blockDim.x + threadIdx.x;
+    const uint64_t Gs = (uint64_t)tm.size * blockDim.x;
     for (uint64_t i = g; i < E; i += Gs) rb.top[G0 + i] = ld_cg_v2(reinterpret_cast<const uint32_t*>(eq + i));
-    if (!grid_barrier(gb)) { res.ok = 0; return res; }
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(rb.top_count, (uint32_t)E);
-    if (!grid_barrier(gb)) res.ok = 0;
+    if (!team_sync(tm)) { res.ok = 0; return res; }
+    if (tm.rank == 0 && threadIdx.x == 0) atomicAdd(rb.top_count, (uint32_t)E);
+    if (!team_sync(tm)) res.ok = 0;
     return res;
   }
   if (E < R) { res.ok = 0; return res; }
@@ -514,8 +669,8 @@ DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_p
   s.pairs = eq;
   s.count_dev = rb.set_count + j + 1;
   Level F0 = radix_level0(8, R);
-  hist_pass<KM>(s, true, true, F0, 256, fb.H[0], s_hist);
-  if (!grid_barrier(gb)) { res.ok = 0; return res; }
+  hist_pass<KM>(tm, s, true, true, F0, 256, fb.H[0], s_hist);
+  if (!team_sync(tm)) { res.ok = 0; return res; }
   RunBufs fr = fb;
   fr.cbuf[0] = rb.cbuf[eqb ^ 1];
   fr.cbuf[1] = rb.cbuf[eqb];
@@ -526,16 +681,16 @@ DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_p
   int eqb2 = 0;
   uint64_t E2 = 0;
   bool ok2 = true;
-  int j2 = run_levels<KM>(fc, s, true, fr, F0, s_hist, gb, Lf2, lp2, eqb2, E2, ok2);
+  int j2 = run_levels<KM>(fc, s, true, fr, F0, s_hist, tm, Lf2, lp2, eqb2, E2, ok2);
   (void)j2;
   if (!ok2 || E2 != 1 || Lf2.R != 1) { res.ok = 0; return res; }
   // append the single remaining entry
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (tm.rank == 0 && threadIdx.x == 0) {
     uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(fr.cbuf[eqb2]));
     uint32_t slot = atomicAdd(rb.top_count, 1u);
     rb.top[slot] = e;
   }
-  if (!grid_barrier(gb)) res.ok = 0;
+  if (!team_sync(tm)) res.ok = 0;
   return res;
 }
 

@@ -1,6 +1,7 @@
 // fused.cuh -- everything after the delegate sampler, in one persistent
-// cooperative kernel with grid barriers between phases (no host round trip;
-// the reference makes ~30 synchronous calls here: radixselect.cuh:1782-1894).
+// kernel with team barriers between phases (no host round trip; the
+// reference makes ~30 synchronous calls here: radixselect.cuh:1782-1894).
+// The team is the cooperative grid, one thread-block cluster, or one CTA.
 //
 //   phase 1  first select on the delegates
 //            default path (beta=1): k-th largest delegate with the reference's
@@ -65,6 +66,7 @@ struct FusedArgs {
   uint32_t* sort_tot;     // [8][256]
   uint32_t* stats;        // [16]
   uint32_t* thr_word;     // threshold handed between launches in split mode
+  uint32_t* tail_flag;    // shared-memory tail: 1 done, 2 fall back to the general path
   int phase_lo, phase_hi; // phases run by this launch of k_fused (1..3)
   GridBar gb;
 };
@@ -83,7 +85,7 @@ DRTOPK_DEV void emit_candidate(const FusedArgs& a, bool take, uint32_t key, uint
     if (slot < a.cand_cap) a.cand[slot] = make_uint2(key, idx);
     else ovf = true;
     if (a.bucket) { mlo = max(mlo, ~key); mhi = max(mhi, key); }
-    else atomicAdd(&s_hist[key >> (32 - a.nbits)], 1u);
+    else hist_add_warp(s_hist, key >> (32 - a.nbits));
   }
 }
 
@@ -106,14 +108,14 @@ DRTOPK_DEV void load4(const FusedArgs& a, uint64_t base, bool vec, uint32_t (&v)
 constexpr int GATHER_U = 8;
 
 template <int KM, int GATHER_U = drtopk::GATHER_U>
-DRTOPK_DEV void gather_list(const FusedArgs& a, const uint2* ids2, const uint32_t* ids1, uint64_t nsub, uint32_t thr,
-                            uint32_t* s_hist, uint32_t& mlo, uint32_t& mhi, bool& ovf) {
+DRTOPK_DEV void gather_list(const Team& tm, const FusedArgs& a, const uint2* ids2, const uint32_t* ids1, uint64_t nsub,
+                            uint32_t thr, uint32_t* s_hist, uint32_t& mlo, uint32_t& mhi, bool& ovf) {
   const uint64_t S = 1ull << a.alpha;
   const int gshift = a.alpha >= 2 ? 2 : a.alpha;  // log2 keys per granule
   const int gk = 1 << gshift;
   const uint64_t units = (nsub * S) >> gshift;
   const uint64_t T = (uint64_t)blockDim.x * GATHER_U;
-  for (uint64_t tb = (uint64_t)blockIdx.x * T; tb < units; tb += (uint64_t)gridDim.x * T) {
+  for (uint64_t tb = (uint64_t)tm.rank * T; tb < units; tb += (uint64_t)tm.size * T) {
     uint32_t v[GATHER_U][4];
     uint32_t base[GATHER_U];  // key index of the granule (n < 2^32)
     uint64_t take = 0;
@@ -158,7 +160,7 @@ DRTOPK_DEV void gather_list(const FusedArgs& a, const uint2* ids2, const uint32_
           else ovf = true;
           ++slot;
           if (a.bucket) { mlo = max(mlo, ~key); mhi = max(mhi, key); }
-          else atomicAdd(&s_hist[key >> (32 - a.nbits)], 1u);
+          else hist_add_warp(s_hist, key >> (32 - a.nbits));
         }
       }
   }
@@ -170,10 +172,10 @@ DRTOPK_DEV void gather_list(const FusedArgs& a, const uint2* ids2, const uint32_
 constexpr int FILTER_E = 8;
 
 template <int KM>
-DRTOPK_DEV void filter_beta(const FusedArgs& a, uint32_t thr, uint32_t* s_hist, uint32_t& mlo, uint32_t& mhi,
-                            bool& ovf) {
+DRTOPK_DEV void filter_beta(const Team& tm, const FusedArgs& a, uint32_t thr, uint32_t* s_hist, uint32_t& mlo,
+                            uint32_t& mhi, bool& ovf) {
   const uint64_t T = (uint64_t)blockDim.x * FILTER_E;
-  for (uint64_t tb = (uint64_t)blockIdx.x * T; tb < a.M; tb += (uint64_t)gridDim.x * T) {
+  for (uint64_t tb = (uint64_t)tm.rank * T; tb < a.M; tb += (uint64_t)tm.size * T) {
     uint32_t m1[FILTER_E];
     uint32_t lon = 0, sel = 0, cl = 0, cs = 0;
 #pragma unroll
@@ -202,7 +204,7 @@ DRTOPK_DEV void filter_beta(const FusedArgs& a, uint32_t thr, uint32_t* s_hist, 
         else ovf = true;
         ++sl.a;
         if (a.bucket) { mlo = max(mlo, ~m1[q]); mhi = max(mhi, m1[q]); }
-        else atomicAdd(&s_hist[m1[q] >> (32 - a.nbits)], 1u);
+        else hist_add_warp(s_hist, m1[q] >> (32 - a.nbits));
       }
       if ((sel >> q) & 1u) a.sel[sl.b++] = (uint32_t)j;
     }
@@ -211,13 +213,13 @@ DRTOPK_DEV void filter_beta(const FusedArgs& a, uint32_t thr, uint32_t* s_hist, 
 
 // min/max pass over a key array (plain bucket path)
 template <int KM>
-DRTOPK_DEV void minmax_pass(const FusedArgs& a, uint32_t* gmm) {
+DRTOPK_DEV void minmax_pass(const Team& tm, const FusedArgs& a, uint32_t* gmm) {
   __shared__ uint32_t s_mm[2];
   if (threadIdx.x < 2) s_mm[threadIdx.x] = 0;
   __syncthreads();
   uint32_t lo = 0, hi = 0;
-  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t g = (uint64_t)tm.rank * blockDim.x + threadIdx.x;
+  const uint64_t G = (uint64_t)tm.size * blockDim.x;
   for (uint64_t i = g; i < a.n; i += G) {
     uint32_t k = to_key<KM>(__ldg(a.keys + i));
     lo = max(lo, ~k);
@@ -254,9 +256,9 @@ DRTOPK_DEV void block_bitonic_desc(uint64_t* s, int npow2) {
 // Each CTA owns one contiguous range; per digit: CTA counts -> column scan
 // over CTAs (one digit column per CTA) -> stable scatter.  Returns the
 // buffer holding the result.
-DRTOPK_DEV uint64_t* grid_lsd_sort(const FusedArgs& a, uint64_t* src, uint64_t* dst, uint32_t nk, uint32_t* s_cnt,
-                                   bool& ok) {
-  const int C = gridDim.x, c = blockIdx.x, t = threadIdx.x;
+DRTOPK_DEV uint64_t* grid_lsd_sort(const Team& tm, const FusedArgs& a, uint64_t* src, uint64_t* dst, uint32_t nk,
+                                   uint32_t* s_cnt, bool& ok) {
+  const int C = (int)tm.size, c = (int)tm.rank, t = threadIdx.x;
   const uint32_t per = (nk + C - 1) / C;
   const uint32_t r0 = min(nk, per * c), r1 = min(nk, r0 + per);
   // totals of all 8 digits
@@ -269,9 +271,9 @@ DRTOPK_DEV uint64_t* grid_lsd_sort(const FusedArgs& a, uint64_t* src, uint64_t* 
       if (s_cnt[i]) atomicAdd(&a.sort_tot[d * 256 + i], s_cnt[i]);
     __syncthreads();
   }
-  if (!grid_barrier(a.gb)) { ok = false; return src; }
+  if (!team_sync(tm)) { ok = false; return src; }
   __shared__ uint32_t s_run[256];
-  __shared__ uint32_t s_wcnt[FUSED_THREADS / 32][257];
+  __shared__ uint32_t s_wcnt[MAX_BLOCK_WARPS][257];
   __shared__ int s_trivial;
   for (int d = 0; d < 8; ++d) {
     if (t == 0) s_trivial = 0;
@@ -287,7 +289,7 @@ DRTOPK_DEV uint64_t* grid_lsd_sort(const FusedArgs& a, uint64_t* src, uint64_t* 
     for (uint32_t i = r0 + t; i < r1; i += blockDim.x) atomicAdd(&s_cnt[(ld_cg_u64(src + i) >> sh) & 255u], 1u);
     __syncthreads();
     for (int i = t; i < 256; i += blockDim.x) a.sort_cnt[(uint64_t)c * 256 + i] = s_cnt[i];
-    if (!grid_barrier(a.gb)) { ok = false; return src; }
+    if (!team_sync(tm)) { ok = false; return src; }
     // 2) exclusive scan of each digit column over the CTAs (in place)
     for (int col = c; col < 256; col += C) {
       if (t < 32) {
@@ -306,7 +308,7 @@ DRTOPK_DEV uint64_t* grid_lsd_sort(const FusedArgs& a, uint64_t* src, uint64_t* 
         }
       }
     }
-    if (!grid_barrier(a.gb)) { ok = false; return src; }
+    if (!team_sync(tm)) { ok = false; return src; }
     // 3) running offsets = digit base (scan of totals) + this CTA's column prefix
     if (t < 256) s_cnt[t] = ld_cg_u32(a.sort_tot + d * 256 + t);
     __syncthreads();
@@ -339,12 +341,12 @@ DRTOPK_DEV uint64_t* grid_lsd_sort(const FusedArgs& a, uint64_t* src, uint64_t* 
       __syncthreads();
       for (int q = t; q < 256; q += blockDim.x) {
         uint32_t add = 0;
-        for (int w2 = 0; w2 < FUSED_THREADS / 32; ++w2) add += s_wcnt[w2][q];
+        for (int w2 = 0; w2 < (int)(blockDim.x / 32); ++w2) add += s_wcnt[w2][q];
         s_run[q] += add;
       }
       __syncthreads();
     }
-    if (!grid_barrier(a.gb)) { ok = false; return src; }
+    if (!team_sync(tm)) { ok = false; return src; }
     uint64_t* tmp = src; src = dst; dst = tmp;
   }
   return src;
@@ -358,14 +360,14 @@ DRTOPK_DEV void stamp(uint32_t* stats, int slot) {
 }
 
 // --------------------------------------------------------------- kernel
+// The phases of one problem, run by one team (the whole cooperative grid,
+// one thread-block cluster, or one CTA).
 template <int KM>
-__global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
-  extern __shared__ __align__(16) uint32_t s_dyn[];
+DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) {
   uint32_t* s_hist = s_dyn;
   // two SMALL_SET-entry buffers after the histogram (runs finished in one CTA)
   uint2* s_fast = reinterpret_cast<uint2*>(s_dyn + ((max(a.nb, 256) + 3) & ~3));
-  const GridBar& gb = a.gb;
-  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  const bool lead = tm.rank == 0 && threadIdx.x == 0;
   const int D = 32 / a.nbits;
   uint32_t thr1 = 0, nsel = 0, nlonely = 0;
   int lvA = 0;
@@ -382,8 +384,8 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
     Level L0;
     if (a.bucket) {
       L0 = bucket_level0(~ld_cg_u32(a.del_minmax), ld_cg_u32(a.del_minmax + 1), a.nb, a.k);
-      hist_pass<KM>(s, false, false, L0, a.nb, a.A.H[0], s_hist);
-      if (!grid_barrier(gb)) return;
+      hist_pass<KM>(tm, s, false, false, L0, a.nb, a.A.H[0], s_hist);
+      if (!team_sync(tm)) return;
     } else {
       L0 = radix_level0(a.nbits, a.k);
     }
@@ -399,7 +401,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
     if (a.path == PATH_BETA && c.max_levels <= 0) {
       thr1 = 0;  // no digit processed: every subrange qualifies
     } else {
-      RunResult r = run_select<KM>(c, s, false, a.A, a.AF, L0, s_hist, gb, s_fast);
+      RunResult r = run_select<KM>(c, s, false, a.A, a.AF, L0, s_hist, tm, s_fast);
       if (!r.ok) { if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL); return; }
       lvA = r.levels;
       // radix keeps the reference's flag (final range lower bound); the bucket
@@ -431,10 +433,10 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
       if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
       return;
     }
-    gather_list<KM>(a, a.A.top, nullptr, a.k, thr1, s_hist, mlo, mhi, ovf);
+    gather_list<KM>(tm, a, a.A.top, nullptr, a.k, thr1, s_hist, mlo, mhi, ovf);
   } else if (a.path == PATH_BETA) {
-    filter_beta<KM>(a, thr1, s_hist, mlo, mhi, ovf);
-    if (!grid_barrier(gb)) return;
+    filter_beta<KM>(tm, a, thr1, s_hist, mlo, mhi, ovf);
+    if (!team_sync(tm)) return;
     const uint32_t nsel_sub = ld_cg_u32(a.sel_count);
     if (lead) {
       a.stats[ST_NSEL] = nsel_sub;
@@ -444,7 +446,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
       if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
       return;
     }
-    gather_list<KM>(a, nullptr, a.sel, nsel_sub, thr1, s_hist, mlo, mhi, ovf);
+    gather_list<KM>(tm, a, nullptr, a.sel, nsel_sub, thr1, s_hist, mlo, mhi, ovf);
   }
   if (ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
   if (a.phase_lo > 2) {
@@ -462,14 +464,14 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
     }
   } else {
     // plain select: level-0 statistics straight off the input
-    if (a.bucket) minmax_pass<KM>(a, a.cand_minmax);
+    if (a.bucket) minmax_pass<KM>(tm, a, a.cand_minmax);
     else {
       Src s = {};
       s.keys = a.keys; s.count = a.n; s.raw_input = 1;
-      hist_pass<KM>(s, false, false, radix_level0(a.nbits, a.k), a.nb, a.C.H[0], s_hist);
+      hist_pass<KM>(tm, s, false, false, radix_level0(a.nbits, a.k), a.nb, a.C.H[0], s_hist);
     }
   }
-  if (!grid_barrier(gb)) return;
+  if (!team_sync(tm)) return;
 
   // ---------------- phase 3: second select
   if (lead) {
@@ -492,15 +494,15 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
   Level L0c;
   if (a.bucket) {
     L0c = bucket_level0(~ld_cg_u32(a.cand_minmax), ld_cg_u32(a.cand_minmax + 1), a.nb, a.k);
-    hist_pass<KM>(sc, pairs, false, L0c, a.nb, a.C.H[0], s_hist);
-    if (!grid_barrier(gb)) return;
+    hist_pass<KM>(tm, sc, pairs, false, L0c, a.nb, a.C.H[0], s_hist);
+    if (!team_sync(tm)) return;
   } else {
     L0c = radix_level0(a.nbits, a.k);
   }
   EngineCfg cc;
   cc.bucket = a.bucket; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
   cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0;
-  RunResult rc = run_select<KM>(cc, sc, pairs, a.C, a.CF, L0c, s_hist, gb, s_fast);
+  RunResult rc = run_select<KM>(cc, sc, pairs, a.C, a.CF, L0c, s_hist, tm, s_fast);
   if (!rc.ok) { if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL); return; }
   const uint32_t K = rc.kth;
   const uint32_t ntop = ld_cg_u32(a.C.top_count);
@@ -522,8 +524,8 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
   if (ntop != a.k) return;
 
   // ---------------- phase 4: top-k output
-  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t g = (uint64_t)tm.rank * blockDim.x + threadIdx.x;
+  const uint64_t G = (uint64_t)tm.size * blockDim.x;
   if (!a.sorted) {
     for (uint64_t i = g; i < a.k; i += G) {
       uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i));
@@ -533,18 +535,13 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
     return;
   }
   if (a.k <= SMALL_SORT) {
-    if (blockIdx.x != 0) return;
+    if (tm.rank != 0) return;
     uint64_t* s = reinterpret_cast<uint64_t*>(s_dyn);
     int np2 = 1;
     while (np2 < (int)a.k) np2 <<= 1;
-    for (int i = threadIdx.x; i < np2; i += blockDim.x) {
-      uint64_t v = 0;
-      if (i < (int)a.k) {
-        uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i));
-        v = ((uint64_t)e.x << 32) | (uint64_t)(~e.y);
-      }
-      s[i] = v;
-    }
+    for (int i = (int)a.k + threadIdx.x; i < np2; i += blockDim.x) s[i] = 0;
+    block_load_loop<8>(a.k, [&](uint32_t i) { return ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i)); },
+                       [&](uint32_t i, uint2 e) { s[i] = ((uint64_t)e.x << 32) | (uint64_t)(~e.y); });
     block_bitonic_desc(s, np2);
     for (int i = threadIdx.x; i < (int)a.k; i += blockDim.x) {
       uint64_t v = s[i];
@@ -558,15 +555,40 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
     uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i));
     a.sort_buf[0][i] = ((uint64_t)(~e.x) << 32) | (uint64_t)e.y;
   }
-  if (!grid_barrier(gb)) return;
+  if (!team_sync(tm)) return;
   bool ok = true;
-  uint64_t* res = grid_lsd_sort(a, a.sort_buf[0], a.sort_buf[1], a.k, s_hist, ok);
+  uint64_t* res = grid_lsd_sort(tm, a, a.sort_buf[0], a.sort_buf[1], a.k, s_hist, ok);
   if (!ok) return;
   for (uint64_t i = g; i < a.k; i += G) {
     const uint64_t v = ld_cg_u64(res + i);
     if (a.out_vals) a.out_vals[i] = from_key(~(uint32_t)(v >> 32), a.km);
     if (a.out_idx) a.out_idx[i] = (int64_t)(uint32_t)v;
   }
+}
+
+// cooperative launch: the whole grid is the team
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  fused_body<KM>(a, grid_team(a.gb), s_dyn);
+}
+
+// cluster launch: every thread-block cluster is the team of one problem --
+// problem clusterid.x of `list`, or the kernel argument when list is null
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_fused_cl(FusedArgs a0, const FusedArgs* list) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  __shared__ FusedArgs s_args;
+  const FusedArgs* ap = &a0;
+  if (list) {
+    const uint32_t cid = cluster_id_x();
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(list + cid);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&s_args);
+    for (int i = threadIdx.x; i < (int)(sizeof(FusedArgs) / 4); i += blockDim.x) dst[i] = __ldg(src + i);
+    __syncthreads();
+    ap = &s_args;
+  }
+  fused_body<KM>(*ap, cluster_team(), s_dyn);
 }
 
 // --------------------------------------------------------------- split mode
@@ -595,7 +617,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_filter(FusedArgs a) {
   clear_hist(s_hist, a.nb);
   uint32_t mlo = 0, mhi = 0;
   bool ovf = false;
-  filter_beta<KM>(a, thr, s_hist, mlo, mhi, ovf);
+  filter_beta<KM>(grid_team(a.gb), a, thr, s_hist, mlo, mhi, ovf);
   if (ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
   flush_cand_stats(a, s_hist, mlo, mhi);
 }
@@ -624,8 +646,9 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_gather(FusedArgs a) {
   clear_hist(s_hist, a.nb);
   uint32_t mlo = 0, mhi = 0;
   bool ovf = false;
-  if (a.path == PATH_DEFAULT) gather_list<KM, 4>(a, a.A.top, nullptr, nsub, thr, s_hist, mlo, mhi, ovf);
-  else gather_list<KM, 4>(a, nullptr, a.sel, nsub, thr, s_hist, mlo, mhi, ovf);
+  const Team tm = grid_team(a.gb);
+  if (a.path == PATH_DEFAULT) gather_list<KM, 4>(tm, a, a.A.top, nullptr, nsub, thr, s_hist, mlo, mhi, ovf);
+  else gather_list<KM, 4>(tm, a, nullptr, a.sel, nsub, thr, s_hist, mlo, mhi, ovf);
   if (ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
   flush_cand_stats(a, s_hist, mlo, mhi);
 }

@@ -14,13 +14,13 @@ namespace drtopk {
 // control block words (zeroed by one memset per call)
 enum CtrlWord : int {
   CW_ERR = 0,
-  CW_BAR_COUNT = 1,
-  CW_BAR_GEN = 2,
+  CW_BAR_COUNT = 1,   // grid barrier word: (generation << 16) | arrivals
   CW_DEL_MINMAX = 4,   // 2 words
   CW_CAND_MINMAX = 6,  // 2 words
   CW_CAND_COUNT = 8,
   CW_SEL_COUNT = 9,
   CW_THR = 10,         // first-select threshold handed between launches
+  CW_TAIL = 11,        // shared-memory tail outcome
   CW_STATS = 16,       // 32 words
   CTRL_HDR_WORDS = 48
 };
@@ -38,6 +38,8 @@ struct Plan {
   uint64_t cand_cap;
   int fused_grid, sample_grid;
   int split;           // concatenation as separate kernels (large inputs)
+  int cluster;         // > 0: phases after the sampler run in one thread-block cluster of this many CTAs
+  int tail;            // 1: phases after the sampler run in one CTA with the sets in shared memory
   int split_grid, filter_grid;
   size_t fused_smem;
   size_t run_words;
@@ -62,5 +64,8 @@ drtopk_status_t plan_select(int device, uint64_t n, uint64_t k, drtopk_dtype_t d
 drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, void* d_kth, void* d_vals,
                                int64_t* d_idx, char* ws, cudaStream_t st, cudaEvent_t* ev);
 int ref_alpha(double log2n, double k);
+// concatenation length (keys) up to which the automatic choice lets one CTA
+// run the phases after the sampler
+constexpr double TAIL_GATHER_AUTO = 32768.0;
 
 }  // namespace drtopk

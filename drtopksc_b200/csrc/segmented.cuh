@@ -42,6 +42,8 @@ struct SegDesc {
   uint64_t out_off;   // first output slot
   uint32_t len, k;
   int32_t km, mode, alpha, ntasks;
+  int32_t sorted;  // 1: this segment's top-k sorted (value desc, index asc)
+  int32_t pad_;
   // optional absolute pointers (served form: every request owns its buffers);
   // when kptr is set the segment's keys are kptr[0..len) and its outputs go
   // to okth[0], ovals[0..k), oidx[0..k) instead of the packed batch arrays
@@ -70,7 +72,6 @@ struct SegArgs {
   uint32_t* out_kth;
   uint32_t* out_vals;
   int64_t* out_idx;
-  int sorted;
 };
 
 DRTOPK_DEV uint32_t to_key_rt(uint32_t u, int km) {
@@ -143,7 +144,7 @@ DRTOPK_DEV uint32_t block_kth(uint64_t n, uint32_t k, G&& get, uint32_t* s_hist,
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const uint64_t i = b + (uint64_t)u * blockDim.x + threadIdx.x;
-        if (i < n && (v[u] & mask_hi) == lo) atomicAdd(&s_hist[(v[u] >> sh) & 255u], 1u);
+        if (i < n && (v[u] & mask_hi) == lo) hist_add_warp(s_hist, (v[u] >> sh) & 255u);
       }
     }
     __syncthreads();
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(SEG_THREADS) k_segmented(SegArgs a) {
     }
     __syncthreads();
     // output (s_top holds the top-k in index order)
-    if (a.sorted) {
+    if (d.sorted) {
       // bitonic sort of composites (key << 32 | ~idx), descending, in place
       uint64_t* c64 = reinterpret_cast<uint64_t*>(s_top);
       int np2 = 1;

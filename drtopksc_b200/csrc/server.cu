@@ -1,18 +1,25 @@
 // server.cu -- served form: continuous batching of top-k requests.
 //
 // A worker thread admits queued requests as in-flight slots and the HBM byte
-// budget allow (device memory from a stream-ordered pool, so admission never
-// synchronises the device), and keeps admitting while earlier requests are
-// still on the GPU:
-//   * requests with n <= 2^22 and k <= 4096 admitted in the same tick are grouped into ONE
-//     persistent segmented launch (segmented.cuh), each segment reading and
-//     writing its request's own buffers; batches rotate over streams 1..7;
-//   * other requests run one select each, in order on stream 0 (their
-//     fused kernel is a cooperative launch that wants the whole GPU, so
-//     they are pipelined rather than raced against each other).
+// budget allow, and keeps admitting while earlier requests are still on the
+// GPU:
+//   * requests with n <= 2^22 and k <= 4096 admitted in the same tick are
+//     grouped into ONE persistent segmented launch (segmented.cuh), each
+//     segment reading and writing its request's own buffers;
+//   * other requests run one select each, in order on their own stream
+//     (their fused kernel may be a cooperative launch: one at a time);
+//   * each request's outputs come back with ONE device-to-host copy on a
+//     third stream, ordered after its kernels by an event, so result copies
+//     never stall the compute streams.
+// Device memory: a request's keys copy and workspace come from the
+// stream-ordered pool and go back on the same compute stream right after its
+// kernels; its outputs come from a per-server cache and go back when its
+// completion event has fired.  The worker holds the server mutex only to
+// move requests between the queue, the admitted set and the result list;
+// CUDA calls run unlocked.
 // Results are exact and identical to the plain call (same kernels / same
-// integer arithmetic); completion is detected with events and results are
-// copied into the caller's host buffers before they are reported by poll().
+// integer arithmetic); results are copied into the caller's host buffers
+// before poll() reports them.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,7 +43,11 @@ using namespace drtopk;
 
 namespace {
 
-constexpr int NSTREAMS = 8;  // stream 0: single selects (cooperative); 1..7: micro-batches
+// stream roles
+constexpr int ST_SINGLE = 0;  // single selects (one in flight at a time)
+constexpr int ST_BATCH = 1;   // micro-batches (segmented kernel, not cooperative)
+constexpr int ST_COPY = 2;    // result copies to pinned host memory and completion events
+constexpr int NSTREAMS = 3;
 constexpr uint64_t BATCH_MAX_N = 1ull << 22;  // larger inputs run as single selects
 
 struct Req {
@@ -49,7 +60,10 @@ struct Req {
   const void* dkeys_user = nullptr;  // device-resident keys (caller-owned)
   void* hkeys = nullptr;             // pinned copy of host keys
   size_t hkeys_cap = 0;
-  char* dmem = nullptr;              // keys copy + outputs (+ workspace for large requests)
+  char* dmem = nullptr;              // keys copy (+ workspace when run alone): stream-ordered, freed
+                                     // on the compute stream right after the request's kernels
+  char* dout = nullptr;              // outputs (kth | values | indices) from the server's device cache
+  size_t dout_cap = 0;
   size_t dbytes = 0;
   size_t ws_bytes = 0;
   uint32_t* d_keys = nullptr;
@@ -63,11 +77,10 @@ struct Req {
   size_t extra_cap = 0;
   cudaEvent_t ev = nullptr;
   int stream = 0;
+  drtopk_result_t res = {};
   double t_submit = 0, t_start = 0, t_done = 0;
   int status = DRTOPK_OK;
   bool small = false;
-  char* batch_ws = nullptr;          // shared batch workspace (freed with the last member)
-  std::shared_ptr<int> batch_refs;
 };
 
 // Process-wide cache of pinned host buffers (size classes of powers of two),
@@ -76,6 +89,8 @@ struct PinnedCache {
   std::mutex mu;
   std::multimap<size_t, void*> free_;
   size_t cached = 0;
+  std::atomic<uint64_t> allocs{0};
+  std::atomic<uint64_t> alloc_ns{0};
   void* get(size_t bytes, size_t* cap) {
     std::lock_guard<std::mutex> lk(mu);
     size_t c = 4096;
@@ -89,7 +104,12 @@ struct PinnedCache {
       return p;
     }
     void* p = nullptr;
-    if (cudaHostAlloc(&p, c, cudaHostAllocPortable) != cudaSuccess) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const cudaError_t e = cudaHostAlloc(&p, c, cudaHostAllocPortable);
+    alloc_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0)
+                    .count();
+    allocs++;
+    if (e != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }
@@ -108,6 +128,41 @@ struct PinnedCache {
   }
 };
 
+// Per-server cache of device output buffers (power-of-two size classes).  A
+// buffer goes back to the cache only after its request's completion event
+// has fired (its result copy is done), so reuse needs no stream ordering.
+struct DevCache {
+  std::multimap<size_t, void*> free_;
+  std::vector<void*> all;
+  void* get(size_t bytes, size_t* cap) {
+    size_t c = 4096;
+    while (c < bytes) c <<= 1;
+    auto it = free_.lower_bound(c);
+    if (it != free_.end() && it->first <= 2 * c) {
+      void* p = it->second;
+      *cap = it->first;
+      free_.erase(it);
+      return p;
+    }
+    void* p = nullptr;
+    if (cudaMalloc(&p, c) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    all.push_back(p);
+    *cap = c;
+    return p;
+  }
+  void put(void* p, size_t cap) {
+    if (p) free_.emplace(cap, p);
+  }
+  void release() {
+    for (void* p : all) cudaFree(p);
+    all.clear();
+    free_.clear();
+  }
+};
+
 PinnedCache& pinned_cache() {
   static PinnedCache* c = new PinnedCache();  // lives until process exit
   return *c;
@@ -123,22 +178,25 @@ struct drtopk_server {
   int max_inflight = 64;
   drtopk_handle_t h = nullptr;
   cudaStream_t streams[NSTREAMS] = {};
-  int next_stream = 0;
+  cudaEvent_t ev_kernels = nullptr;  // kernels-done marker (re-recorded per launch)
   int seg_grid = 0;
   size_t seg_smem = 0;
   std::mutex mu;
   std::condition_variable cv, done_cv;
-  std::deque<Req*> queue;
-  std::list<Req*> running;
+  std::deque<Req*> queue;           // guarded by mu
+  std::list<Req*> running;          // worker thread only
   std::deque<drtopk_result_t> results;
   size_t used = 0;
-  int inflight = 0;
+  int inflight = 0;                 // admitted, not yet published (guarded by mu)
   uint64_t next_id = 1;
   bool stop = false;
   std::thread worker;
   std::chrono::steady_clock::time_point t0;
   PinnedCache& pinned = pinned_cache();
-  std::vector<cudaEvent_t> ev_free;
+  DevCache outs;                    // worker thread only
+  std::vector<cudaEvent_t> ev_free; // worker thread only
+  drtopk_server_stats_t stats = {}; // guarded by mu
+  uint64_t pin_allocs0 = 0, pin_ns0 = 0;
 
   double now_ms() const {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -175,17 +233,21 @@ struct drtopk_server {
     *out = b;
     return DRTOPK_OK;
   }
-  void complete(Req* r, cudaError_t q);
-  void admit_and_launch();
+  void copy_out(Req* r, cudaError_t q);
+  void publish(Req* r);
+  void finish_on_copy_stream(Req* r, cudaEvent_t kernels_done);
+  void admit(std::vector<Req*>& out);
+  void launch_admitted(std::vector<Req*>& v);
   void launch_single(Req* r);
   void launch_batch(std::vector<Req*>& v, int si);
   void loop();
 };
 
-void drtopk_server::complete(Req* r, cudaError_t q) {
+// result of a finished request into the caller's buffers (worker thread, unlocked)
+void drtopk_server::copy_out(Req* r, cudaError_t q) {
   r->t_done = now_ms();
   if (q != cudaSuccess) r->status = DRTOPK_ECUDA;
-  drtopk_result_t res;
+  drtopk_result_t& res = r->res;
   std::memset(&res, 0, sizeof(res));
   res.id = r->id;
   if (r->status == DRTOPK_OK) {
@@ -198,18 +260,39 @@ void drtopk_server::complete(Req* r, cudaError_t q) {
   res.t_submit_ms = r->t_submit;
   res.t_start_ms = r->t_start;
   res.t_done_ms = r->t_done;
-  results.push_back(res);
-  used -= r->dbytes;
-  inflight--;
   pinned.put(r->hkeys, r->hkeys_cap);
   pinned.put(r->hout, r->hout_cap);
   pinned.put(r->extra, r->extra_cap);
+  r->hkeys = r->hout = r->extra = nullptr;
+  outs.put(r->dout, r->dout_cap);
+  r->dout = nullptr;
   if (r->ev) ev_free.push_back(r->ev);
+  r->ev = nullptr;
+}
+
+// hand a finished request to poll() (mutex held)
+void drtopk_server::publish(Req* r) {
+  results.push_back(r->res);
+  used -= r->dbytes;
+  inflight--;
   delete r;
 }
 
+// result copy: one D2H of the request's contiguous output block (kth,
+// values, indices when asked) on the copy stream after the kernels, then the
+// completion event
+void drtopk_server::finish_on_copy_stream(Req* r, cudaEvent_t kernels_done) {
+  cudaStream_t xs = streams[ST_COPY];
+  cudaStreamWaitEvent(xs, kernels_done, 0);
+  if (r->status == DRTOPK_OK && r->dout) {
+    const size_t outb = al256(4) + al256(r->k * 4) + (r->user_idx ? al256(r->k * 8) : 0);
+    if (cudaMemcpyAsync(r->hout, r->d_kth, outb, cudaMemcpyDeviceToHost, xs) != cudaSuccess) r->status = DRTOPK_ECUDA;
+  }
+  cudaEventRecord(r->ev, xs);
+}
+
 void drtopk_server::launch_single(Req* r) {
-  cudaStream_t st = streams[r->stream];
+  cudaStream_t st = streams[ST_SINGLE];
   drtopk_params_t p;
   drtopk_params_default(&p);
   p.alpha = -2;  // autotuned parameters
@@ -218,17 +301,12 @@ void drtopk_server::launch_single(Req* r) {
   if (!r->dkeys_user && cudaMemcpyAsync(r->d_keys, r->hkeys, r->n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
     r->status = DRTOPK_ECUDA;
   if (r->status == DRTOPK_OK)
-    r->status = drtopk_select_ws(h, keys, r->dtype, r->n, r->k, &p, r->d_kth, r->d_vals, r->d_idx, r->d_ws,
-                                 r->ws_bytes, st);
-  if (r->status == DRTOPK_OK) {
-    char* ho = static_cast<char*>(r->hout);
-    cudaMemcpyAsync(ho, r->d_kth, 4, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(ho + al256(4), r->d_vals, r->k * 4, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(ho + al256(4) + al256(r->k * 4), r->d_idx, r->k * 8, cudaMemcpyDeviceToHost, st);
-  }
-  cudaFreeAsync(r->dmem, st);
+    r->status = drtopk_select_ws(h, keys, r->dtype, r->n, r->k, &p, r->d_kth, r->d_vals,
+                                 r->user_idx ? r->d_idx : nullptr, r->d_ws, r->ws_bytes, st);
+  if (r->dmem) cudaFreeAsync(r->dmem, st);  // same stream: reusable by the next request at once
   r->dmem = nullptr;
-  cudaEventRecord(r->ev, st);
+  cudaEventRecord(ev_kernels, st);
+  finish_on_copy_stream(r, ev_kernels);
 }
 
 void drtopk_server::launch_batch(std::vector<Req*>& v, int si) {
@@ -248,7 +326,8 @@ void drtopk_server::launch_batch(std::vector<Req*>& v, int si) {
     d.kptr = r->dkeys_user ? static_cast<const uint32_t*>(r->dkeys_user) : r->d_keys;
     d.okth = r->d_kth;
     d.ovals = r->d_vals;
-    d.oidx = r->d_idx;
+    d.oidx = r->user_idx ? r->d_idx : nullptr;
+    d.sorted = r->sorted;
     // same per-segment choice as the batched form
     if (d.len <= 32768) {
       d.mode = SEG_PLAIN;
@@ -311,37 +390,33 @@ void drtopk_server::launch_batch(std::vector<Req*>& v, int si) {
     a.err = ctrl + 1;
     a.done = ctrl + 8;
     a.seg_err = ctrl + 8 + nseg;
-    a.sorted = v[0]->sorted;
     const int grid = std::min<int>(seg_grid, (int)(tasks.size() + nseg));
     if (launch_segmented(a, std::max(1, grid), seg_smem, st) != cudaSuccess) ok = false;
-    for (Req* r : v) {
-      char* ho = static_cast<char*>(r->hout);
-      cudaMemcpyAsync(ho, r->d_kth, 4, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(ho + al256(4), r->d_vals, r->k * 4, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(ho + al256(4) + al256(r->k * 4), r->d_idx, r->k * 8, cudaMemcpyDeviceToHost, st);
-    }
     cudaFreeAsync(ws, st);
   }
   for (Req* r : v) {
-    if (!ok) r->status = DRTOPK_ENOMEM;
-    cudaFreeAsync(r->dmem, st);
+    if (r->dmem) cudaFreeAsync(r->dmem, st);
     r->dmem = nullptr;
-    cudaEventRecord(r->ev, st);
   }
-  // the descriptor staging buffer may be reused only after the copy ran:
-  // it is released with the last request of the batch (same stream)
+  cudaEventRecord(ev_kernels, st);
+  for (Req* r : v) {
+    if (!ok) r->status = DRTOPK_ENOMEM;
+    finish_on_copy_stream(r, ev_kernels);
+  }
+  // the descriptor staging buffer may be reused only after its copy ran:
+  // it is released with the last request of the batch (completion event
+  // recorded later on the copy stream)
   if (hst) {
     v.back()->extra = hst;
     v.back()->extra_cap = hcap;
   }
 }
 
-void drtopk_server::admit_and_launch() {
-  std::vector<Req*> small;
+// Admission (mutex held): move requests from the queue into `out` while the
+// in-flight limit and the byte budget allow; no CUDA calls here.
+void drtopk_server::admit(std::vector<Req*>& out) {
   int scanned = 0;
   const double t = now_ms();
-  // this tick's micro-batch stream: its requests' buffers are allocated on it
-  const int bs = 1 + next_stream % (NSTREAMS - 1);
   for (auto it = queue.begin(); it != queue.end() && inflight < max_inflight && scanned < 256; ++scanned) {
     Req* r = *it;
     size_t need = 0;
@@ -351,10 +426,10 @@ void drtopk_server::admit_and_launch() {
       it = queue.erase(it);
       r->status = s;
       r->t_start = t;
-      inflight++;
-      used += 0;
       r->dbytes = 0;
-      complete(r, cudaSuccess);
+      inflight++;
+      copy_out(r, cudaSuccess);
+      publish(r);
       continue;
     }
     if (budget && used + need > budget) {
@@ -369,68 +444,97 @@ void drtopk_server::admit_and_launch() {
     r->dbytes = need;
     used += need;
     inflight++;
+    out.push_back(r);
+  }
+}
+
+// Device work of the admitted requests (worker thread, unlocked): small
+// requests of this tick form one micro-batch, the others run one select each.
+void drtopk_server::launch_admitted(std::vector<Req*>& v) {
+  std::vector<Req*> small;
+  for (Req* r : v) {
     r->ev = get_event();
     const size_t outb = al256(4) + al256(r->k * 4) + al256(r->k * 8);
     r->hout = pinned.get(outb, &r->hout_cap);
-    r->stream = r->small ? bs : 0;
+    r->stream = r->small ? ST_BATCH : ST_SINGLE;
     cudaStream_t st = streams[r->stream];
-    size_t dev = need;
-    if (r->small) dev = (r->dkeys_user ? 0 : al256(r->n * 4)) + outb;  // batch workspace is separate
-    if (!r->hout || cudaMallocAsync(reinterpret_cast<void**>(&r->dmem), dev, st) != cudaSuccess) {
+    // keys copy (host mode) and, for a request run alone, its workspace
+    const size_t kb = r->dkeys_user ? 0 : al256(r->n * 4);
+    const size_t dev = kb + (r->small ? 0 : al256(r->ws_bytes));
+    running.push_back(r);
+    r->dout = static_cast<char*>(r->hout ? outs.get(outb, &r->dout_cap) : nullptr);
+    if (!r->dout || (dev && cudaMallocAsync(reinterpret_cast<void**>(&r->dmem), dev, st) != cudaSuccess)) {
       cudaGetLastError();
+      r->dmem = nullptr;
       r->status = DRTOPK_ENOMEM;
-      cudaEventRecord(r->ev, st);
-      running.push_back(r);
+      cudaEventRecord(r->ev, streams[ST_COPY]);
       continue;
     }
-    char* p = r->dmem;
-    if (!r->dkeys_user) {
-      r->d_keys = reinterpret_cast<uint32_t*>(p);
-      p += al256(r->n * 4);
-    }
+    if (!r->dkeys_user) r->d_keys = reinterpret_cast<uint32_t*>(r->dmem);
+    r->d_ws = r->dmem + kb;
+    char* p = r->dout;
     r->d_kth = reinterpret_cast<uint32_t*>(p);
     p += al256(4);
     r->d_vals = reinterpret_cast<uint32_t*>(p);
     p += al256(r->k * 4);
     r->d_idx = reinterpret_cast<int64_t*>(p);
-    p += al256(r->k * 8);
-    r->d_ws = p;
-    running.push_back(r);
     if (r->small) small.push_back(r);
     else launch_single(r);
   }
-  if (!small.empty()) {
-    launch_batch(small, bs);
-    next_stream = (next_stream + 1) % (NSTREAMS - 1);
-  }
+  if (!small.empty()) launch_batch(small, ST_BATCH);
 }
 
 void drtopk_server::loop() {
   cudaSetDevice(device);
-  std::unique_lock<std::mutex> lk(mu);
-  while (true) {
-    if (stop && queue.empty() && running.empty()) break;
-    bool progressed = false;
+  std::vector<Req*> admitted, finished;
+  std::vector<cudaError_t> fq;
+  for (;;) {
+    // completions (running is owned by this thread)
+    finished.clear();
+    fq.clear();
     for (auto it = running.begin(); it != running.end();) {
       cudaError_t q = cudaEventQuery((*it)->ev);
       if (q == cudaErrorNotReady) {
         ++it;
         continue;
       }
-      Req* r = *it;
+      if (q != cudaSuccess) cudaGetLastError();
+      finished.push_back(*it);
+      fq.push_back(q);
       it = running.erase(it);
-      complete(r, q);
-      progressed = true;
     }
-    const size_t before = queue.size();
-    if (!queue.empty()) admit_and_launch();
-    if (queue.size() != before) progressed = true;
-    if (progressed) done_cv.notify_all();
-    if (!progressed) {
-      if (running.empty() && queue.empty())
-        cv.wait_for(lk, std::chrono::milliseconds(5));
-      else
-        cv.wait_for(lk, std::chrono::microseconds(20));
+    const auto tc0 = std::chrono::steady_clock::now();
+    for (size_t i = 0; i < finished.size(); ++i) copy_out(finished[i], fq[i]);
+    const double ms_complete =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc0).count();
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      stats.host_ms_complete += ms_complete;
+      for (Req* r : finished) publish(r);
+      if (stop && queue.empty() && inflight == 0) break;
+      if (!queue.empty()) admit(admitted);
+      if (!finished.empty() || inflight == 0) done_cv.notify_all();
+      if (finished.empty() && admitted.empty()) {
+        if (inflight == 0 && queue.empty())
+          cv.wait_for(lk, std::chrono::milliseconds(5));
+        else
+          cv.wait_for(lk, std::chrono::microseconds(20));
+        continue;
+      }
+    }
+    const auto tl0 = std::chrono::steady_clock::now();
+    uint64_t ns = 0, nbr = 0;
+    for (Req* r : admitted) (r->small ? nbr : ns)++;
+    if (!admitted.empty()) launch_admitted(admitted);
+    admitted.clear();
+    const double ms_launch = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl0).count();
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stats.host_ms_launch += ms_launch;
+      stats.singles += ns;
+      stats.batches += nbr ? 1 : 0;
+      stats.batched += nbr;
+      stats.worker_ticks++;
     }
   }
   done_cv.notify_all();
@@ -452,6 +556,8 @@ extern "C" drtopk_status_t drtopk_server_create(drtopk_server_t* out, int device
   drtopk_status_t st = drtopk_create(&s->h, device, 0);
   for (int i = 0; st == DRTOPK_OK && i < NSTREAMS; ++i)
     if (cudaStreamCreateWithFlags(&s->streams[i], cudaStreamNonBlocking) != cudaSuccess) st = DRTOPK_ECUDA;
+  if (st == DRTOPK_OK && cudaEventCreateWithFlags(&s->ev_kernels, cudaEventDisableTiming) != cudaSuccess)
+    st = DRTOPK_ECUDA;
   if (st == DRTOPK_OK) {
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -465,9 +571,12 @@ extern "C" drtopk_status_t drtopk_server_create(drtopk_server_t* out, int device
     if (s->h) drtopk_destroy(s->h);
     for (auto& x : s->streams)
       if (x) cudaStreamDestroy(x);
+    if (s->ev_kernels) cudaEventDestroy(s->ev_kernels);
     delete s;
     return st;
   }
+  s->pin_allocs0 = s->pinned.allocs.load();
+  s->pin_ns0 = s->pinned.alloc_ns.load();
   s->worker = std::thread([s]() { s->loop(); });
   *out = s;
   return DRTOPK_OK;
@@ -492,9 +601,11 @@ extern "C" drtopk_status_t drtopk_server_destroy(drtopk_server_t s) {
   cudaSetDevice(s->device);
   for (auto& x : s->streams)
     if (x) cudaStreamSynchronize(x);
+  s->outs.release();
   for (auto& x : s->streams)
     if (x) cudaStreamDestroy(x);
   for (auto e : s->ev_free) cudaEventDestroy(e);
+  if (s->ev_kernels) cudaEventDestroy(s->ev_kernels);
   drtopk_destroy(s->h);
   cudaSetDevice(cur);
   delete s;
@@ -593,7 +704,7 @@ extern "C" drtopk_status_t drtopk_server_cancel(drtopk_server_t s, uint64_t id) 
 extern "C" drtopk_status_t drtopk_server_drain(drtopk_server_t s, int timeout_ms) {
   if (!s) return DRTOPK_EINVAL;
   std::unique_lock<std::mutex> lk(s->mu);
-  auto pred = [&]() { return s->queue.empty() && s->running.empty(); };
+  auto pred = [&]() { return s->queue.empty() && s->inflight == 0; };
   if (timeout_ms < 0) {
     s->done_cv.wait(lk, pred);
     return DRTOPK_OK;
@@ -607,5 +718,15 @@ extern "C" drtopk_status_t drtopk_server_usage(drtopk_server_t s, size_t* reside
   if (resident_bytes) *resident_bytes = s->used;
   if (inflight) *inflight = s->inflight;
   if (queued) *queued = (int)s->queue.size();
+  return DRTOPK_OK;
+}
+
+extern "C" drtopk_status_t drtopk_server_stats(drtopk_server_t s, drtopk_server_stats_t* st) {
+  if (!s || !st) return DRTOPK_EINVAL;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *st = s->stats;
+  // the staging cache is process-wide: report what it did since this server started
+  st->pinned_allocs = s->pinned.allocs.load() - s->pin_allocs0;
+  st->host_ms_pinned = (double)(s->pinned.alloc_ns.load() - s->pin_ns0) * 1e-6;
   return DRTOPK_OK;
 }

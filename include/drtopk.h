@@ -65,6 +65,9 @@ typedef struct {
   int largest;      /* 1: k largest (reference semantics, default); 0: k smallest */
   int sorted;       /* 1: top-k sorted by key (best first), ties by index ascending */
   int first_digits; /* beta path: digits used by the first select; 0: reference (32/nbits-3) */
+  int team;         /* CTAs running the phases after the sampler: 0 auto, 1 the whole GPU
+                       (cooperative grid), 2 one thread-block cluster, 3 one CTA with the sets
+                       in shared memory (small problems) */
 } drtopk_params_t;
 
 typedef struct {
@@ -84,6 +87,8 @@ typedef struct {
   double ms_concat;
   double ms_second;
   double ms_total;
+  int team_ctas;             /* CTAs that ran the phases after the sampler */
+  int team_cluster;          /* 0: the cooperative grid; 1: one thread-block cluster; 3: one CTA */
 } drtopk_stats_t;
 
 typedef struct drtopk_handle* drtopk_handle_t;
@@ -260,6 +265,19 @@ DRTOPK_API drtopk_status_t drtopk_server_cancel(drtopk_server_t s, uint64_t id);
 DRTOPK_API drtopk_status_t drtopk_server_drain(drtopk_server_t s, int timeout_ms);
 /* Current resident bytes and in-flight request count. */
 DRTOPK_API drtopk_status_t drtopk_server_usage(drtopk_server_t s, size_t* resident_bytes, int* inflight, int* queued);
+
+/* Counters of the server's worker since creation (observability). */
+typedef struct {
+  uint64_t singles;          /* requests run as one select each */
+  uint64_t batches;          /* micro-batch launches */
+  uint64_t batched;          /* requests run inside micro-batches */
+  uint64_t pinned_allocs;    /* pinned host buffers newly allocated (staging-cache misses) */
+  uint64_t worker_ticks;     /* worker loop iterations that admitted or completed something */
+  double host_ms_pinned;     /* worker time spent allocating pinned staging */
+  double host_ms_launch;     /* worker time issuing device work */
+  double host_ms_complete;   /* worker time copying results to the callers' buffers */
+} drtopk_server_stats_t;
+DRTOPK_API drtopk_status_t drtopk_server_stats(drtopk_server_t s, drtopk_server_stats_t* st);
 
 #ifdef __cplusplus
 }
