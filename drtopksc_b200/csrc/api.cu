@@ -1031,6 +1031,34 @@ extern "C" drtopk_status_t drtopk_profile_end(drtopk_handle_t h, double* ms_samp
 //                                 candidate; a threshold of d digits admits
 //                                 an extra ~2^-8d of the keys (truncation).
 // Subrange counts per bucket follow Poisson(lambda = q' S).
+// Measured delegate-sampler throughput as a fraction of the HBM copy
+// bandwidth on B200 (n = 2^27, no index output), by log2 subrange size alpha
+// (entries 0..16; alpha < 5 is not run on the one-delegate path).  Small
+// subranges cost more instructions per key (lane-owned reductions, and the
+// (Max, Second) pair for beta = 2); float keys pay their order-preserving
+// mapping.  Below ~4096 subranges the warp-per-subrange pass does not fill
+// the GPU, which the occupancy factor models.
+static double sampler_eff(int alpha, bool beta2, bool f32, double M) {
+  static const double u32_b1[17] = {.6, .6, .6, .6, .7, .82, .94, 1, 1, 1, 1, 1, 1, 1, .97, .97, .97};
+  static const double u32_b2[17] = {.5, .5, .53, .75, .8, .8, .94, .93, .89, .97, 1, 1, 1, 1, .97, .97, .97};
+  static const double f32_b1[17] = {.6, .6, .6, .6, .7, .82, .93, .9, .87, .98, .98, .98, .98, .98, .95, .95, .95};
+  static const double f32_b2[17] = {.45, .45, .49, .64, .76, .77, .79, .77, .73, .83, .97, .97, .97, .97, .92, .92, .92};
+  const int a = std::max(0, std::min(alpha, 16));
+  double e = beta2 ? (f32 ? f32_b2[a] : u32_b2[a]) : (f32 ? f32_b1[a] : u32_b1[a]);
+  if (alpha >= 9) e *= 0.7 + 0.3 * std::min(1.0, M / 4096.0);
+  return e;
+}
+
+// Tail calibration (bytes at the HBM roofline): the phases after the sampler
+// run at roughly a third of the copy bandwidth (appends, level barriers), and
+// each path has a fixed part -- the one-delegate path's exact first select
+// over the delegates costs ~20 us, growing to ~70 us once it must keep
+// >= ~1K subranges, the beta path's threshold-only first select ~20 us
+// (measured on B200 at n = 2^27 and 2^30).
+constexpr double TAIL_BYTES_PER_US = 6.55e6;
+static double tail_default(double n, double k, double S);
+static double tail_beta(double n, double k, double S, int digits);
+
 static double cost_default(double n, double k, double S) {
   const double M = n / S;
   return 8.0 * M + 4.0 * k * S + 24.0 * k;
@@ -1044,6 +1072,13 @@ static double cost_beta(double n, double k, double S, int digits) {
   const double p_lone = lam * e;
   const double cand = M * p_lone + M * p_sel * (lam + 1.0);
   return 16.0 * M + 8.0 * M * (digits - 1) + 2.0 * M * p_sel * 4.0 * S + 24.0 * cand;
+}
+
+static double tail_default(double n, double k, double S) {
+  return 3.3 * cost_default(n, k, S) + (20.0 + 50.0 * std::min(1.0, k / 1024.0)) * TAIL_BYTES_PER_US;
+}
+static double tail_beta(double n, double k, double S, int digits) {
+  return 2.8 * cost_beta(n, k, S, digits) + 20.0 * TAIL_BYTES_PER_US;
 }
 
 extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_t dtype, drtopk_params_t* p) {
@@ -1070,8 +1105,10 @@ extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_
   for (int alpha = 2; alpha <= 16; ++alpha) {
     const double S = std::ldexp(1.0, alpha);
     const uint64_t M = (n + (1ull << alpha) - 1) >> alpha;
+    const bool f32 = dtype == DRTOPK_F32;
     if (alpha >= 2 && M >= k) {
-      const double c = cost_default(dn, dk, S);
+      // the sampler's pass over the keys (at its measured speed) plus the tail
+      const double c = 4.0 * dn / sampler_eff(alpha, false, f32, (double)M) + tail_default(dn, dk, S);
       if (c < best) { best = c; best_alpha = alpha; best_path = 1; best_digits = 0; }
     }
     if (2 * M >= k && p->beta == 2) {
@@ -1080,7 +1117,8 @@ extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_
       const int maxd = p->nbits == 8 ? 2 : 1;
       const int mind = (p->nbits == 8 && dtype == DRTOPK_F32) ? 2 : 1;
       for (int d = mind; d <= maxd; ++d) {
-        const double c = cost_beta(dn, dk, S, p->nbits == 8 ? d : (32 / p->nbits - 3));
+        const double c = 4.0 * dn / sampler_eff(alpha, true, f32, (double)M) +
+                         tail_beta(dn, dk, S, p->nbits == 8 ? d : (32 / p->nbits - 3));
         if (c < best) { best = c; best_alpha = alpha; best_path = 2; best_digits = d; }
       }
     }

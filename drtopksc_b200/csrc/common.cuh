@@ -15,9 +15,16 @@ namespace drtopk {
 // largest-first machinery returns the k smallest.
 enum KeyMode : int { KM_U32 = 0, KM_F32 = 1, KM_U32_MIN = 2, KM_F32_MIN = 3 };
 
+// float bits -> order-preserving key without a branch: negative values are
+// inverted (xor with all ones), non-negative ones get the sign bit set
+DRTOPK_DEV uint32_t f32_bits_to_key(uint32_t u) {
+  const uint32_t neg = (uint32_t)((int32_t)u >> 31);  // all ones for negative values
+  return u ^ (neg | 0x80000000u);
+}
+
 template <int KM>
 DRTOPK_DEV uint32_t to_key(uint32_t u) {
-  if (KM == KM_F32 || KM == KM_F32_MIN) u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+  if (KM == KM_F32 || KM == KM_F32_MIN) u = f32_bits_to_key(u);
   if (KM == KM_U32_MIN || KM == KM_F32_MIN) u = ~u;
   return u;
 }

@@ -71,12 +71,15 @@ DRTOPK_DEV Acc acc_shfl_xor(const Acc& s, int off) {
   return o;
 }
 
+// Four consecutive words [base, base+4).  A full row is returned RAW (the
+// caller maps it to keys when it uses it, so the load can stay in flight
+// meanwhile); a partial row is returned as keys, with positions >= n read
+// as key 0 (the max identity).
 template <int KM>
 DRTOPK_DEV void load_row4(const SampleArgs& a, uint64_t base, uint64_t pol, bool full, uint32_t (&k)[4]) {
-  // four consecutive keys [base, base+4); keys >= n read as 0 (the max identity)
   if (full) {
     uint4 v = ld_stream_v4(a.keys + base, pol);
-    k[0] = to_key<KM>(v.x); k[1] = to_key<KM>(v.y); k[2] = to_key<KM>(v.z); k[3] = to_key<KM>(v.w);
+    k[0] = v.x; k[1] = v.y; k[2] = v.z; k[3] = v.w;
   } else {
 #pragma unroll
     for (int e = 0; e < 4; ++e) k[e] = (base + e < a.n) ? to_key<KM>(ld_stream_u32(a.keys + base + e, pol)) : 0u;
@@ -147,10 +150,19 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
         uint32_t k[4][4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) load_row4<KM>(a, c + r * 128 + lane * 4, pol, full, k[r]);
+        // full rows hold raw words (mapped here, after all four loads were issued)
+        if (full) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+          for (int r = 0; r < 4; ++r)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) acc_push<BETA, POS>(s, k[r][q], (uint32_t)(c - b) + r * 128 + lane * 4 + q);
+            for (int q = 0; q < 4; ++q)
+              acc_push<BETA, POS>(s, to_key<KM>(k[r][q]), (uint32_t)(c - b) + r * 128 + lane * 4 + q);
+        } else {
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc_push<BETA, POS>(s, k[r][q], (uint32_t)(c - b) + r * 128 + lane * 4 + q);
+        }
       }
 #pragma unroll
       for (int off = 1; off < 32; off <<= 1) acc_merge<BETA, POS>(s, acc_shfl_xor<BETA, POS>(s, off));
@@ -180,6 +192,9 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
     uint32_t* stage = s_stage[wib];
     const int grp = lane / G, gl = lane % G;
     auto uidx = [&](int i) { return grp * 4 * G + gl + G * i; };  // uint4 index inside the chunk
+    // a full chunk is kept as raw words while its loads are in flight and
+    // mapped to keys when it is reduced; a partial (last) chunk is mapped at
+    // load time, with positions >= n as key 0
     auto load_chunk = [&](uint64_t ch, uint32_t (&k)[4][4]) {
       const uint64_t cb = ch << 9;
       const bool full = a.vec_ok && (cb + 512 <= a.n);
@@ -188,7 +203,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
         const uint64_t base = cb + 4 * (uint64_t)uidx(i);
         if (full) {
           uint4 v = ld_l1_v4(a.keys + base, pol);
-          k[i][0] = to_key<KM>(v.x); k[i][1] = to_key<KM>(v.y); k[i][2] = to_key<KM>(v.z); k[i][3] = to_key<KM>(v.w);
+          k[i][0] = v.x; k[i][1] = v.y; k[i][2] = v.z; k[i][3] = v.w;
         } else {
 #pragma unroll
           for (int e = 0; e < 4; ++e) k[i][e] = (base + e < a.n) ? to_key<KM>(ld_stream_u32(a.keys + base + e, pol)) : 0u;
@@ -200,6 +215,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
     uint64_t ch = gwarp;
     if (ch < nchunks) load_chunk(ch, kn);
     for (; ch < nchunks; ch += nwarps) {
+      const bool full = a.vec_ok && ((ch << 9) + 512 <= a.n);
       uint32_t k[4][4];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
@@ -207,6 +223,12 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
         for (int e = 0; e < 4; ++e) k[i][e] = kn[i][e];
       const uint64_t chn = ch + nwarps;
       if (chn < nchunks) load_chunk(chn, kn);
+      if (full) {  // map this chunk's raw words now that the next chunk's loads are issued
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) k[i][e] = to_key<KM>(k[i][e]);
+      }
       if (alpha >= 4) {
         Acc acc = {0u, 0u, 0u};
 #pragma unroll

@@ -75,7 +75,7 @@ struct SegArgs {
 };
 
 DRTOPK_DEV uint32_t to_key_rt(uint32_t u, int km) {
-  if (km == KM_F32 || km == KM_F32_MIN) u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+  if (km == KM_F32 || km == KM_F32_MIN) u = f32_bits_to_key(u);
   if (km == KM_U32_MIN || km == KM_F32_MIN) u = ~u;
   return u;
 }
