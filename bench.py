@@ -251,9 +251,10 @@ def bench_served(D, torch, dev, stream, args):
            "requests": R, "pool_arrays": npool, "loop_req_per_s": loop_rps,
            "loop_p50_ms": float(np.percentile(lat_loop, 50)), "loop_p99_ms": float(np.percentile(lat_loop, 99)),
            "rates": []}
-    # warm-up: one unmeasured pass (pinned staging cache, memory pool growth)
+    # warm-up: one unmeasured pass over the request list (pinned staging and
+    # device output caches, memory pool growth), as a long-running server has
     srv = D.Server(dev.index or 0, hbm_budget_bytes=120 << 30, max_inflight=64)
-    for (t, n, dt, k) in reqs[:400]:
+    for (t, n, dt, k) in reqs:
         srv.submit(t, k, want_indices=False)
     srv.drain(120000)
     srv.poll(1000)

@@ -128,40 +128,49 @@ struct PinnedCache {
   }
 };
 
-// Per-server cache of device output buffers (power-of-two size classes).  A
-// buffer goes back to the cache only after its request's completion event
-// has fired (its result copy is done), so reuse needs no stream ordering.
+// Process-wide cache of device output buffers, one per device (power-of-two
+// size classes).  A buffer goes back to the cache only after its request's
+// completion event has fired (its result copy is done), so reuse needs no
+// stream ordering; servers created later reuse what earlier ones allocated,
+// so a new server does not pay cudaMalloc in the middle of its traffic.
 struct DevCache {
+  std::mutex mu;
   std::multimap<size_t, void*> free_;
-  std::vector<void*> all;
   void* get(size_t bytes, size_t* cap) {
     size_t c = 4096;
     while (c < bytes) c <<= 1;
-    auto it = free_.lower_bound(c);
-    if (it != free_.end() && it->first <= 2 * c) {
-      void* p = it->second;
-      *cap = it->first;
-      free_.erase(it);
-      return p;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = free_.lower_bound(c);
+      if (it != free_.end() && it->first <= 2 * c) {
+        void* p = it->second;
+        *cap = it->first;
+        free_.erase(it);
+        return p;
+      }
     }
     void* p = nullptr;
-    if (cudaMalloc(&p, c) != cudaSuccess) {
+    if (cudaMalloc(&p, c) != cudaSuccess) {  // on the calling thread's current device
       cudaGetLastError();
       return nullptr;
     }
-    all.push_back(p);
     *cap = c;
     return p;
   }
   void put(void* p, size_t cap) {
-    if (p) free_.emplace(cap, p);
-  }
-  void release() {
-    for (void* p : all) cudaFree(p);
-    all.clear();
-    free_.clear();
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(mu);
+    free_.emplace(cap, p);
   }
 };
+
+DevCache& dev_cache(int device) {
+  static std::mutex mu;
+  static DevCache* caches[64] = {};
+  std::lock_guard<std::mutex> lk(mu);
+  if (!caches[device]) caches[device] = new DevCache();  // lives until process exit
+  return *caches[device];
+}
 
 PinnedCache& pinned_cache() {
   static PinnedCache* c = new PinnedCache();  // lives until process exit
@@ -193,7 +202,7 @@ struct drtopk_server {
   std::thread worker;
   std::chrono::steady_clock::time_point t0;
   PinnedCache& pinned = pinned_cache();
-  DevCache outs;                    // worker thread only
+  DevCache* outs = nullptr;         // this device's process-wide output cache
   std::vector<cudaEvent_t> ev_free; // worker thread only
   drtopk_server_stats_t stats = {}; // guarded by mu
   uint64_t pin_allocs0 = 0, pin_ns0 = 0;
@@ -264,7 +273,7 @@ void drtopk_server::copy_out(Req* r, cudaError_t q) {
   pinned.put(r->hout, r->hout_cap);
   pinned.put(r->extra, r->extra_cap);
   r->hkeys = r->hout = r->extra = nullptr;
-  outs.put(r->dout, r->dout_cap);
+  outs->put(r->dout, r->dout_cap);
   r->dout = nullptr;
   if (r->ev) ev_free.push_back(r->ev);
   r->ev = nullptr;
@@ -462,7 +471,7 @@ void drtopk_server::launch_admitted(std::vector<Req*>& v) {
     const size_t kb = r->dkeys_user ? 0 : al256(r->n * 4);
     const size_t dev = kb + (r->small ? 0 : al256(r->ws_bytes));
     running.push_back(r);
-    r->dout = static_cast<char*>(r->hout ? outs.get(outb, &r->dout_cap) : nullptr);
+    r->dout = static_cast<char*>(r->hout ? outs->get(outb, &r->dout_cap) : nullptr);
     if (!r->dout || (dev && cudaMallocAsync(reinterpret_cast<void**>(&r->dmem), dev, st) != cudaSuccess)) {
       cudaGetLastError();
       r->dmem = nullptr;
@@ -546,10 +555,11 @@ extern "C" drtopk_status_t drtopk_server_create(drtopk_server_t* out, int device
   *out = nullptr;
   int cur = 0;
   cudaGetDevice(&cur);
-  if (cudaSetDevice(device) != cudaSuccess) return DRTOPK_EINVAL;
+  if (device < 0 || device >= 64 || cudaSetDevice(device) != cudaSuccess) return DRTOPK_EINVAL;
   drtopk_server* s = new (std::nothrow) drtopk_server();
   if (!s) return DRTOPK_ENOMEM;
   s->device = device;
+  s->outs = &dev_cache(device);
   s->budget = hbm_budget_bytes;
   s->max_inflight = max_inflight > 0 ? max_inflight : 64;
   s->t0 = std::chrono::steady_clock::now();
@@ -601,7 +611,6 @@ extern "C" drtopk_status_t drtopk_server_destroy(drtopk_server_t s) {
   cudaSetDevice(s->device);
   for (auto& x : s->streams)
     if (x) cudaStreamSynchronize(x);
-  s->outs.release();
   for (auto& x : s->streams)
     if (x) cudaStreamDestroy(x);
   for (auto e : s->ev_free) cudaEventDestroy(e);
