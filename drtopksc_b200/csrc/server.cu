@@ -6,8 +6,10 @@
 //   * requests with n <= 2^22 and k <= 4096 admitted in the same tick are
 //     grouped into ONE persistent segmented launch (segmented.cuh), each
 //     segment reading and writing its request's own buffers;
-//   * other requests run one select each, in order on their own stream
-//     (their fused kernel may be a cooperative launch: one at a time);
+//   * other requests run one select each: in order on one stream when their
+//     tail is the cooperative whole-GPU kernel (one at a time), on a second
+//     stream when it is the one-CTA shared-memory tail, which then overlaps
+//     the other streams' work;
 //   * each request's outputs come back with ONE device-to-host copy on a
 //     third stream, ordered after its kernels by an event, so result copies
 //     never stall the compute streams.
@@ -37,6 +39,7 @@
 #include <vector>
 
 #include "../../include/drtopk.h"
+#include "plan.h"
 #include "segmented.cuh"
 
 using namespace drtopk;
@@ -44,10 +47,12 @@ using namespace drtopk;
 namespace {
 
 // stream roles
-constexpr int ST_SINGLE = 0;  // single selects (one in flight at a time)
+constexpr int ST_SINGLE = 0;  // single selects whose tail is a cooperative launch (one at a time)
 constexpr int ST_BATCH = 1;   // micro-batches (segmented kernel, not cooperative)
 constexpr int ST_COPY = 2;    // result copies to pinned host memory and completion events
-constexpr int NSTREAMS = 3;
+constexpr int ST_TAIL = 3;    // single selects with the one-CTA shared-memory tail (not cooperative),
+                              // overlapping the other streams' work on the device
+constexpr int NSTREAMS = 4;
 constexpr uint64_t BATCH_MAX_N = 1ull << 22;  // larger inputs run as single selects
 
 struct Req {
@@ -301,7 +306,7 @@ void drtopk_server::finish_on_copy_stream(Req* r, cudaEvent_t kernels_done) {
 }
 
 void drtopk_server::launch_single(Req* r) {
-  cudaStream_t st = streams[ST_SINGLE];
+  cudaStream_t st = streams[r->stream];
   drtopk_params_t p;
   drtopk_params_default(&p);
   p.alpha = -2;  // autotuned parameters
@@ -466,6 +471,17 @@ void drtopk_server::launch_admitted(std::vector<Req*>& v) {
     const size_t outb = al256(4) + al256(r->k * 4) + al256(r->k * 8);
     r->hout = pinned.get(outb, &r->hout_cap);
     r->stream = r->small ? ST_BATCH : ST_SINGLE;
+    if (!r->small) {
+      // a select whose tail is the one-CTA kernel holds few SMs and never
+      // waits on other CTAs: it runs on its own stream, beside the others
+      drtopk_params_t p;
+      drtopk_params_default(&p);
+      p.alpha = -2;
+      p.sorted = r->sorted;
+      Plan P;
+      if (plan_select(device, r->n, r->k, r->dtype, &p, r->user_idx != nullptr, &P) == DRTOPK_OK && P.tail)
+        r->stream = ST_TAIL;
+    }
     cudaStream_t st = streams[r->stream];
     // keys copy (host mode) and, for a request run alone, its workspace
     const size_t kb = r->dkeys_user ? 0 : al256(r->n * 4);
