@@ -632,6 +632,9 @@ static RunBufs run_bufs(char* ctrl, const Plan& P, int which) {
   r.res = base + 3 * P.hist_words + MAX_LEVELS + 2 + 1;
   r.cbuf[0] = r.cbuf[1] = nullptr;
   r.top = nullptr;
+  r.top_cap = 0;
+  r.cbuf_cap = 0;
+  r.err = reinterpret_cast<uint32_t*>(ctrl) + CW_ERR;
   return r;
 }
 
@@ -767,6 +770,12 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
   a.sorted = P.sorted;
   a.cand = reinterpret_cast<uint2*>(ws + P.off_cand);
   a.cand_cap = P.cand_cap;
+  a.C.top_cap = a.CF.top_cap = P.k;
+  a.C.cbuf_cap = a.CF.cbuf_cap = P.cand_cap;
+  if (P.path == PATH_DEFAULT) {
+    a.A.top_cap = a.AF.top_cap = P.k;
+    a.A.cbuf_cap = a.AF.cbuf_cap = P.M;
+  }
   a.C.top = reinterpret_cast<uint2*>(ws + P.off_Ctop);
   a.C.cbuf[0] = reinterpret_cast<uint2*>(ws + P.off_Ccbuf0);
   a.C.cbuf[1] = a.cand;  // level >= 1 may overwrite the candidates

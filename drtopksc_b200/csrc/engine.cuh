@@ -49,6 +49,9 @@ struct RunBufs {
   uint2* top;           // top list (capacity k)
   uint32_t* top_count;
   uint32_t* res;        // [4] result of a run finished inside one CTA: thr, kth, levels, ok
+  uint64_t top_cap;     // entries the top list holds
+  uint64_t cbuf_cap;    // entries each compact buffer holds
+  uint32_t* err;        // error word: DE_OVERFLOW when an append would pass a capacity
 };
 
 struct Level {
@@ -159,6 +162,28 @@ DRTOPK_DEV bool advance(const EngineCfg& c, const Level& L, const Pick& p, int l
 }
 
 // --------------------------------------------------------------- helpers
+// Team-strided loop over [0, n) with U loads per thread in flight: ld(i) for
+// every index of a round, then use(i, value).  Consecutive threads take
+// consecutive indices within each of the U slices (coalesced).
+template <int U, typename LD, typename USE>
+DRTOPK_DEV void team_load_loop(const Team& tm, uint64_t n, LD&& ld, USE&& use) {
+  using V = decltype(ld(uint64_t(0)));
+  const uint64_t G = (uint64_t)tm.size * blockDim.x;
+  for (uint64_t b = (uint64_t)tm.rank * blockDim.x + threadIdx.x; b < n; b += G * U) {
+    V v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint64_t i = b + (uint64_t)u * G;
+      if (i < n) v[u] = ld(i);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint64_t i = b + (uint64_t)u * G;
+      if (i < n) use(i, v[u]);
+    }
+  }
+}
+
 DRTOPK_DEV void zero_words(const Team& tm, uint32_t* p, int n) {
   const uint64_t g = (uint64_t)tm.rank * blockDim.x + threadIdx.x;
   const uint64_t G = (uint64_t)tm.size * blockDim.x;
@@ -224,8 +249,10 @@ constexpr int SPLIT_E = 16;  // entries per thread per tile
 template <int KM>
 DRTOPK_DEV void split_tiles(const Team& tm, const EngineCfg& c, const Src& s, bool pairs, uint64_t count,
                             const Level& N, bool want_hist, uint2* top, uint32_t* top_count, uint2* nxt,
-                            uint32_t* nxt_count, uint32_t* s_hist) {
+                            uint32_t* nxt_count, uint32_t* s_hist, uint64_t top_cap, uint64_t nxt_cap,
+                            uint32_t* err) {
   const uint64_t T = (uint64_t)blockDim.x * SPLIT_E;
+  bool ovf = false;
   for (uint64_t tb = (uint64_t)tm.rank * T; tb < count; tb += (uint64_t)tm.size * T) {
     uint32_t val[SPLIT_E], pay[SPLIT_E];
     uint32_t up = 0, in = 0, ca = 0, cb = 0;
@@ -258,14 +285,23 @@ DRTOPK_DEV void split_tiles(const Team& tm, const EngineCfg& c, const Src& s, bo
     Slots2 sl = block_append2(ca, cb, top_count, nxt_count);
 #pragma unroll
     for (int e = 0; e < SPLIT_E; ++e) {
-      if ((up >> e) & 1u) top[sl.a++] = make_uint2(val[e], pay[e]);
+      // the histogram bounds both counts; a capacity check still guards
+      // every address computed from device data
+      if ((up >> e) & 1u) {
+        if (sl.a < top_cap) top[sl.a] = make_uint2(val[e], pay[e]);
+        else ovf = true;
+        ++sl.a;
+      }
       if ((in >> e) & 1u) {
-        nxt[sl.b++] = make_uint2(val[e], pay[e]);
+        if (sl.b < nxt_cap) nxt[sl.b] = make_uint2(val[e], pay[e]);
+        else ovf = true;
+        ++sl.b;
         const uint32_t key = c.key_from_payload ? ~pay[e] : val[e];
         if (want_hist) hist_add_warp(s_hist, bin_of(key, N.lo, N.w, N.wshift));
       }
     }
   }
+  if (ovf && err) atomicOr(err, (uint32_t)DE_OVERFLOW);
 }
 
 // --------------------------------------------------------------- one run
@@ -314,7 +350,7 @@ DRTOPK_DEV int run_levels(const EngineCfg& c, const Src& src0, bool src0_pairs, 
       cnt = ld_cg_u32(rb.set_count + j);
     }
     split_tiles<KM>(tm, c, s, from_pairs, cnt, N, want_hist, rb.top, rb.top_count, rb.cbuf[j & 1],
-                    rb.set_count + j + 1, s_hist);
+                    rb.set_count + j + 1, s_hist, rb.top_cap, rb.cbuf_cap, rb.err);
     if (want_hist) flush_hist(s_hist, Hn, c.nb);
     if (!team_sync(tm)) { ok = false; break; }
     L = N;
@@ -466,7 +502,8 @@ DRTOPK_DEV Pick smem_level_pick(const uint2* sA, uint32_t n, const Level& L, int
 // contiguous runs ranked by ballots: no shared-memory bank conflicts, index
 // order kept.  Ends with a block barrier.
 DRTOPK_DEV void split_block(const uint2* src, uint32_t n, uint32_t lo, uint32_t hi, bool want_a, uint2* outA,
-                            uint32_t* cntA, uint2* outB, uint32_t* cntB) {
+                            uint32_t* cntA, uint2* outB, uint32_t* cntB, uint64_t capA = ~0ull,
+                            uint32_t* err = nullptr) {
   __shared__ uint32_t s_wa[32], s_wb[32], s_base[2];
   const unsigned lane = threadIdx.x & 31u;
   const int w = threadIdx.x >> 5, W = blockDim.x >> 5;
@@ -507,7 +544,11 @@ DRTOPK_DEV void split_block(const uint2* src, uint32_t n, uint32_t lo, uint32_t 
     const bool ia = v && want_a && e.x > hi;
     const bool ib = v && e.x >= lo && e.x <= hi;
     const unsigned ma = __ballot_sync(0xffffffffu, ia), mb = __ballot_sync(0xffffffffu, ib);
-    if (ia) outA[pa + __popc(ma & lt)] = e;
+    if (ia) {
+      const uint32_t slot = pa + __popc(ma & lt);
+      if (slot < capA) outA[slot] = e;
+      else if (err) atomicOr(err, (uint32_t)DE_OVERFLOW);
+    }
     if (ib) outB[pb + __popc(mb & lt)] = e;
     pa += __popc(ma);
     pb += __popc(mb);
@@ -541,7 +582,7 @@ DRTOPK_DEV void block_finish(const EngineCfg& c, const Src& src, bool pairs, uin
     if (p.cnt != n) {  // else the whole set is in the chosen bin: nothing moves
       if (threadIdx.x == 0) s_n = 0;
       __syncthreads();
-      split_block(sA, n, N.lo, N.hi, true, rb.top, rb.top_count, sB, &s_n);
+      split_block(sA, n, N.lo, N.hi, true, rb.top, rb.top_count, sB, &s_n, rb.top_cap, rb.err);
       n = s_n;
       uint2* t = sA; sA = sB; sB = t;
     }
@@ -555,7 +596,10 @@ DRTOPK_DEV void block_finish(const EngineCfg& c, const Src& src, bool pairs, uin
   if (ok && n == R) {
     if (threadIdx.x == 0) s_tb = atomicAdd(rb.top_count, n);
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) rb.top[s_tb + i] = sA[i];
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+      if ((uint64_t)s_tb + i < rb.top_cap) rb.top[s_tb + i] = sA[i];
+      else if (rb.err) atomicOr(rb.err, (uint32_t)DE_OVERFLOW);
+    }
   } else if (ok && n > R) {
     // keep the R lowest payloads among the tied entries
     uint64_t* w = reinterpret_cast<uint64_t*>(sB);
@@ -566,8 +610,10 @@ DRTOPK_DEV void block_finish(const EngineCfg& c, const Src& src, bool pairs, uin
     block_bitonic_asc(w, np2);
     if (threadIdx.x == 0) s_tb = atomicAdd(rb.top_count, R);
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < R; i += blockDim.x)
-      rb.top[s_tb + i] = make_uint2((uint32_t)w[i], (uint32_t)(w[i] >> 32));
+    for (uint32_t i = threadIdx.x; i < R; i += blockDim.x) {
+      if ((uint64_t)s_tb + i < rb.top_cap) rb.top[s_tb + i] = make_uint2((uint32_t)w[i], (uint32_t)(w[i] >> 32));
+      else if (rb.err) atomicOr(rb.err, (uint32_t)DE_OVERFLOW);
+    }
   } else {
     ok = false;
   }
@@ -656,7 +702,12 @@ DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_p
     const uint64_t G0 = (uint64_t)ld_cg_u32(rb.top_count);
     const uint64_t g = (uint64_t)tm.rank * blockDim.x + threadIdx.x;
     const uint64_t Gs = (uint64_t)tm.size * blockDim.x;
-    for (uint64_t i = g; i < E; i += Gs) rb.top[G0 + i] = ld_cg_v2(reinterpret_cast<const uint32_t*>(eq + i));
+    (void)g; (void)Gs;
+    team_load_loop<8>(tm, E, [&](uint64_t i) { return ld_cg_v2(reinterpret_cast<const uint32_t*>(eq + i)); },
+                      [&](uint64_t i, uint2 v) {
+                        if (G0 + i < rb.top_cap) rb.top[G0 + i] = v;
+                        else if (rb.err) atomicOr(rb.err, (uint32_t)DE_OVERFLOW);
+                      });
     if (!team_sync(tm)) { res.ok = 0; return res; }
     if (tm.rank == 0 && threadIdx.x == 0) atomicAdd(rb.top_count, (uint32_t)E);
     if (!team_sync(tm)) res.ok = 0;
@@ -676,6 +727,9 @@ DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_p
   fr.cbuf[1] = rb.cbuf[eqb];
   fr.top = rb.top;
   fr.top_count = rb.top_count;
+  fr.top_cap = rb.top_cap;
+  fr.cbuf_cap = rb.cbuf_cap;
+  fr.err = rb.err;
   Level Lf2;
   Pick lp2;
   int eqb2 = 0;

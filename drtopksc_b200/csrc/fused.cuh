@@ -265,7 +265,8 @@ DRTOPK_DEV uint64_t* grid_lsd_sort(const Team& tm, const FusedArgs& a, uint64_t*
   for (int d = 0; d < 8; ++d) {
     for (int i = t; i < 256; i += blockDim.x) s_cnt[i] = 0;
     __syncthreads();
-    for (uint32_t i = r0 + t; i < r1; i += blockDim.x) atomicAdd(&s_cnt[(ld_cg_u64(src + i) >> (8 * d)) & 255u], 1u);
+    block_load_loop<8>(r1 - r0, [&](uint32_t i) { return ld_cg_u64(src + r0 + i); },
+                       [&](uint32_t, uint64_t v) { atomicAdd(&s_cnt[(v >> (8 * d)) & 255u], 1u); });
     __syncthreads();
     for (int i = t; i < 256; i += blockDim.x)
       if (s_cnt[i]) atomicAdd(&a.sort_tot[d * 256 + i], s_cnt[i]);
@@ -286,7 +287,8 @@ DRTOPK_DEV uint64_t* grid_lsd_sort(const Team& tm, const FusedArgs& a, uint64_t*
     // 1) this CTA's digit counts
     for (int i = t; i < 256; i += blockDim.x) s_cnt[i] = 0;
     __syncthreads();
-    for (uint32_t i = r0 + t; i < r1; i += blockDim.x) atomicAdd(&s_cnt[(ld_cg_u64(src + i) >> sh) & 255u], 1u);
+    block_load_loop<8>(r1 - r0, [&](uint32_t i) { return ld_cg_u64(src + r0 + i); },
+                       [&](uint32_t, uint64_t v) { atomicAdd(&s_cnt[(v >> sh) & 255u], 1u); });
     __syncthreads();
     for (int i = t; i < 256; i += blockDim.x) a.sort_cnt[(uint64_t)c * 256 + i] = s_cnt[i];
     if (!team_sync(tm)) { ok = false; return src; }
@@ -527,11 +529,11 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
   const uint64_t g = (uint64_t)tm.rank * blockDim.x + threadIdx.x;
   const uint64_t G = (uint64_t)tm.size * blockDim.x;
   if (!a.sorted) {
-    for (uint64_t i = g; i < a.k; i += G) {
-      uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i));
-      if (a.out_vals) a.out_vals[i] = from_key(e.x, a.km);
-      if (a.out_idx) a.out_idx[i] = (int64_t)e.y;
-    }
+    team_load_loop<8>(tm, a.k, [&](uint64_t i) { return ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i)); },
+                      [&](uint64_t i, uint2 e) {
+                        if (a.out_vals) a.out_vals[i] = from_key(e.x, a.km);
+                        if (a.out_idx) a.out_idx[i] = (int64_t)e.y;
+                      });
     return;
   }
   if (a.k <= SMALL_SORT) {
@@ -551,19 +553,17 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
     return;
   }
   // large k: multi-CTA stable LSD radix sort of (~key << 32 | index)
-  for (uint64_t i = g; i < a.k; i += G) {
-    uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i));
-    a.sort_buf[0][i] = ((uint64_t)(~e.x) << 32) | (uint64_t)e.y;
-  }
+  team_load_loop<8>(tm, a.k, [&](uint64_t i) { return ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i)); },
+                    [&](uint64_t i, uint2 e) { a.sort_buf[0][i] = ((uint64_t)(~e.x) << 32) | (uint64_t)e.y; });
   if (!team_sync(tm)) return;
   bool ok = true;
   uint64_t* res = grid_lsd_sort(tm, a, a.sort_buf[0], a.sort_buf[1], a.k, s_hist, ok);
   if (!ok) return;
-  for (uint64_t i = g; i < a.k; i += G) {
-    const uint64_t v = ld_cg_u64(res + i);
+  (void)g; (void)G;
+  team_load_loop<8>(tm, a.k, [&](uint64_t i) { return ld_cg_u64(res + i); }, [&](uint64_t i, uint64_t v) {
     if (a.out_vals) a.out_vals[i] = from_key(~(uint32_t)(v >> 32), a.km);
     if (a.out_idx) a.out_idx[i] = (int64_t)(uint32_t)v;
-  }
+  });
 }
 
 // cooperative launch: the whole grid is the team
