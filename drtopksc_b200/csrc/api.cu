@@ -10,13 +10,16 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <new>
 #include <vector>
 
 #include "../../include/drtopk.h"
 #include "bitonic.cuh"
 #include "fused.cuh"
+#include "kernels.h"
 #include "plan.h"
 #include "tail.cuh"
 #include "sampler.cuh"
@@ -45,7 +48,7 @@ static cudaError_t dev_info(int device, DevInfo** out) {
     cudaError_t e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
     int occ = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sample<KM_U32, 2, true>, SAMPLE_THREADS, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernels(KM_U32).sample2pos, SAMPLE_THREADS, 0);
     if (e != cudaSuccess) return e;
     d.occ_sample = std::max(1, occ);
     d.device = device;
@@ -54,31 +57,9 @@ static cudaError_t dev_info(int device, DevInfo** out) {
   return cudaSuccess;
 }
 
-template <int KM>
-static void* fused_fn() {
-  return (void*)k_fused<KM>;
-}
-static void* fused_ptr(int km) {
-  switch (km) {
-    case KM_U32: return fused_fn<KM_U32>();
-    case KM_F32: return fused_fn<KM_F32>();
-    case KM_U32_MIN: return fused_fn<KM_U32_MIN>();
-    default: return fused_fn<KM_F32_MIN>();
-  }
-}
+static void* fused_ptr(int km) { return const_cast<void*>(kernels(km).fused); }
 
-template <int KM>
-static void* fused_cl_fn() {
-  return (void*)k_fused_cl<KM>;
-}
-static void* fused_cl_ptr(int km) {
-  switch (km) {
-    case KM_U32: return fused_cl_fn<KM_U32>();
-    case KM_F32: return fused_cl_fn<KM_F32>();
-    case KM_U32_MIN: return fused_cl_fn<KM_U32_MIN>();
-    default: return fused_cl_fn<KM_F32_MIN>();
-  }
-}
+static void* fused_cl_ptr(int km) { return const_cast<void*>(kernels(km).fused_cl); }
 
 // Largest cluster (16, else 8, else 4) of k_fused_cl CTAs that the device
 // can co-schedule with the largest dynamic shared memory a plan uses
@@ -119,18 +100,7 @@ static int cluster_size(DevInfo* d, int km, size_t smem) {
   return c > 0 ? c : 0;
 }
 
-template <int KM>
-static void* tail_fn() {
-  return (void*)k_tail<KM>;
-}
-static void* tail_ptr(int km) {
-  switch (km) {
-    case KM_U32: return tail_fn<KM_U32>();
-    case KM_F32: return tail_fn<KM_F32>();
-    case KM_U32_MIN: return tail_fn<KM_U32_MIN>();
-    default: return tail_fn<KM_F32_MIN>();
-  }
-}
+static void* tail_ptr(int km) { return const_cast<void*>(kernels(km).tail); }
 static cudaLaunchConfig_t tail_config(cudaStream_t st, cudaLaunchAttribute* at) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(TAIL_CLUSTER);
@@ -167,30 +137,33 @@ static bool tail_ready(int device, int km) {
   return s > 0;
 }
 
-template <int KM>
-static void* filter_fn() {
-  return (void*)k_filter<KM>;
-}
-template <int KM>
-static void* gather_fn() {
-  return (void*)k_gather<KM>;
-}
-static void* split_ptr(int km, bool filter) {
-  switch (km) {
-    case KM_U32: return filter ? filter_fn<KM_U32>() : gather_fn<KM_U32>();
-    case KM_F32: return filter ? filter_fn<KM_F32>() : gather_fn<KM_F32>();
-    case KM_U32_MIN: return filter ? filter_fn<KM_U32_MIN>() : gather_fn<KM_U32_MIN>();
-    default: return filter ? filter_fn<KM_F32_MIN>() : gather_fn<KM_F32_MIN>();
+// the ordinary (non-cooperative) kernels of split mode
+enum SplitKernel : int { SK_GATHER = 0, SK_FILTER = 1, SK_LEVEL_HIST = 2, SK_SPLIT0 = 3 };
+static void* split_ptr(int km, int which) {
+  const KernelSet& ks = kernels(km);
+  switch (which) {
+    case SK_FILTER: return const_cast<void*>(ks.filter);
+    case SK_LEVEL_HIST: return const_cast<void*>(ks.level_hist);
+    case SK_SPLIT0: return const_cast<void*>(ks.split0);
+    default: return const_cast<void*>(ks.gather);
   }
 }
 
-static cudaError_t split_grid(DevInfo* d, int km, bool filter, size_t smem, int* grid) {
-  static int occ_cache[64][4][2];
+// dynamic shared memory of a split-mode kernel: histogram words + warp stages
+static size_t split_smem(int nb, int which) {
+  const size_t h = (size_t)std::max(nb, 256) * 4;
+  return which == SK_FILTER ? h + SPLIT_FILTER_SMEM : (which == SK_GATHER ? h + SPLIT_GATHER_SMEM : h);
+}
+
+static cudaError_t split_grid(DevInfo* d, int km, int which, size_t smem, int* grid) {
+  static std::map<std::tuple<int, int, int, size_t>, int> occ_cache;
   std::lock_guard<std::mutex> lk(g_dev_mu);
-  int& occ = occ_cache[d->device][km][filter ? 1 : 0];
+  int& occ = occ_cache[std::make_tuple(d->device, km, which, smem)];
   if (occ == 0) {
+    cudaError_t e = cudaFuncSetAttribute(split_ptr(km, which), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     int o = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, split_ptr(km, filter), FUSED_THREADS, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, split_ptr(km, which), FUSED_THREADS, smem);
     if (e != cudaSuccess) return e;
     occ = std::max(1, o);
   }
@@ -213,18 +186,7 @@ static cudaError_t fused_max_grid(DevInfo* d, int km, size_t smem, int* grid) {
   return cudaSuccess;
 }
 
-template <int KM>
-static void* bitonic_fn() {
-  return (void*)k_bitonic<KM>;
-}
-static void* bitonic_ptr(int km) {
-  switch (km) {
-    case KM_U32: return bitonic_fn<KM_U32>();
-    case KM_F32: return bitonic_fn<KM_F32>();
-    case KM_U32_MIN: return bitonic_fn<KM_U32_MIN>();
-    default: return bitonic_fn<KM_F32_MIN>();
-  }
-}
+static void* bitonic_ptr(int km) { return const_cast<void*>(kernels(km).bitonic); }
 
 static cudaError_t bitonic_max_grid(DevInfo* d, int km, size_t smem, int* grid) {
   static int occ_cache[64][4];
@@ -521,10 +483,16 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
   if (P->path == PATH_BETA || P->path == PATH_DEFAULT) {
     const uint64_t concat = P->path == PATH_BETA ? P->M * 8 : k * P->S * 4;
     P->split = concat >= (16ull << 20) ? 1 : 0;
-    const size_t hs = (size_t)std::max(P->nb, 256) * 4;
-    if (P->split && (split_grid(di, P->km, true, hs, &P->filter_grid) != cudaSuccess ||
-                     split_grid(di, P->km, false, hs, &P->split_grid) != cudaSuccess))
+    if (P->split && (split_grid(di, P->km, SK_FILTER, split_smem(P->nb, SK_FILTER), &P->filter_grid) != cudaSuccess ||
+                     split_grid(di, P->km, SK_GATHER, split_smem(P->nb, SK_GATHER), &P->split_grid) != cudaSuccess ||
+                     split_grid(di, P->km, SK_LEVEL_HIST, split_smem(P->nb, SK_LEVEL_HIST), &P->hist_grid) !=
+                         cudaSuccess ||
+                     split_grid(di, P->km, SK_SPLIT0, split_smem(P->nb, SK_SPLIT0), &P->split0_grid) != cudaSuccess))
       return DRTOPK_ECUDA;
+    // the beta path's threshold-only first select (radix, <= 2 levels) needs
+    // no cooperative launch: its one histogram pass is k_level_hist and the
+    // picks are made by every k_filter CTA
+    P->first_pre = (P->split && P->path == PATH_BETA && !P->bucket && P->first_levels <= 2) ? 1 : 0;
   }
   // team of the phases after the sampler: one CTA with the sets in shared
   // memory when they are small (their cost is then round trips, not
@@ -562,7 +530,7 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
       P->cluster = cluster_size(di, P->km, smem);
       if (P->cluster <= 0) return DRTOPK_EUNSUPPORTED;
     }
-    if (P->tail || P->cluster) P->split = 0;
+    if (P->tail || P->cluster) P->split = P->first_pre = 0;
   }
   // sampler grid: persistent, capped by the work items
   if (P->path != PATH_PLAIN && !(P->path == PATH_BITONIC && P->normal)) {
@@ -610,15 +578,11 @@ extern "C" drtopk_status_t drtopk_workspace_size(uint64_t n, uint64_t k, drtopk_
 // ------------------------------------------------------------ launch
 namespace drtopk {
 
-template <int KM>
-static cudaError_t launch_sample(const SampleArgs& sa, int beta, bool pos, int grid, cudaStream_t st) {
-  if (beta == 2) {
-    if (pos) k_sample<KM, 2, true><<<grid, SAMPLE_THREADS, 0, st>>>(sa);
-    else k_sample<KM, 2, false><<<grid, SAMPLE_THREADS, 0, st>>>(sa);
-  } else {
-    k_sample<KM, 1, false><<<grid, SAMPLE_THREADS, 0, st>>>(sa);
-  }
-  return cudaGetLastError();
+static cudaError_t launch_sample(int km, SampleArgs sa, int beta, bool pos, int grid, cudaStream_t st) {
+  const KernelSet& ks = kernels(km);
+  const void* fn = beta == 2 ? (pos ? ks.sample2pos : ks.sample2) : ks.sample1;
+  void* args[] = {&sa};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(SAMPLE_THREADS), args, 0, st);
 }
 
 static RunBufs run_bufs(char* ctrl, const Plan& P, int which) {
@@ -635,16 +599,14 @@ static RunBufs run_bufs(char* ctrl, const Plan& P, int which) {
   r.top_cap = 0;
   r.cbuf_cap = 0;
   r.err = reinterpret_cast<uint32_t*>(ctrl) + CW_ERR;
+  r.out_km = 0;
+  r.out_vals = nullptr;
+  r.out_idx = nullptr;
   return r;
 }
 
 static cudaError_t launch_sampler_km(const Plan& P, const SampleArgs& sa, int beta, cudaStream_t st) {
-  switch (P.km) {
-    case KM_U32: return launch_sample<KM_U32>(sa, beta, P.has_pos, P.sample_grid, st);
-    case KM_F32: return launch_sample<KM_F32>(sa, beta, P.has_pos, P.sample_grid, st);
-    case KM_U32_MIN: return launch_sample<KM_U32_MIN>(sa, beta, P.has_pos, P.sample_grid, st);
-    default: return launch_sample<KM_F32_MIN>(sa, beta, P.has_pos, P.sample_grid, st);
-  }
+  return launch_sample(P.km, sa, beta, P.has_pos, P.sample_grid, st);
 }
 
 static drtopk_status_t launch_coop(void* fn, const Plan& P, void* argp, cudaStream_t st) {
@@ -777,6 +739,9 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
     a.A.cbuf_cap = a.AF.cbuf_cap = P.M;
   }
   a.C.top = reinterpret_cast<uint2*>(ws + P.off_Ctop);
+  a.C.out_km = P.km;
+  a.C.out_vals = a.out_vals;
+  a.C.out_idx = d_idx;
   a.C.cbuf[0] = reinterpret_cast<uint2*>(ws + P.off_Ccbuf0);
   a.C.cbuf[1] = a.cand;  // level >= 1 may overwrite the candidates
   if (P.path == PATH_DEFAULT) {
@@ -827,18 +792,38 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
     s = launch_coop(fused_ptr(P.km), P, &a, st);
   } else {
     a.phase_hi = 1;
-    s = launch_coop(fused_ptr(P.km), P, &a, st);
-    const size_t smem = (size_t)std::max(P.nb, 256) * 4;
+    if (P.first_pre) {
+      a.first_pre = 1;
+      s = DRTOPK_OK;
+      if (P.first_levels >= 2) {
+        void* args[] = {&a};
+        if (cudaLaunchKernel(split_ptr(P.km, SK_LEVEL_HIST), dim3(P.hist_grid), dim3(FUSED_THREADS), args,
+                             split_smem(P.nb, SK_LEVEL_HIST), st) != cudaSuccess)
+          s = DRTOPK_ECUDA;
+      }
+    } else {
+      s = launch_coop(fused_ptr(P.km), P, &a, st);
+    }
     if (s == DRTOPK_OK && P.path == PATH_BETA) {
       void* args[] = {&a};
-      if (cudaLaunchKernel(split_ptr(P.km, true), dim3(P.filter_grid), dim3(FUSED_THREADS), args, smem, st) !=
-          cudaSuccess)
+      if (cudaLaunchKernel(split_ptr(P.km, SK_FILTER), dim3(P.filter_grid), dim3(FUSED_THREADS), args,
+                           split_smem(P.nb, SK_FILTER), st) != cudaSuccess)
         s = DRTOPK_ECUDA;
     }
     if (s == DRTOPK_OK) {
       void* args[] = {&a};
-      if (cudaLaunchKernel(split_ptr(P.km, false), dim3(P.split_grid), dim3(FUSED_THREADS), args, smem, st) !=
-          cudaSuccess)
+      if (cudaLaunchKernel(split_ptr(P.km, SK_GATHER), dim3(P.split_grid), dim3(FUSED_THREADS), args,
+                           split_smem(P.nb, SK_GATHER), st) != cudaSuccess)
+        s = DRTOPK_ECUDA;
+    }
+    if (s == DRTOPK_OK && !P.bucket) {
+      // level 0 of the second select as an ordinary kernel; unsorted
+      // output is written by it directly
+      a.split0 = 1;
+      a.direct0 = P.sorted ? 0 : 1;
+      void* args[] = {&a};
+      if (cudaLaunchKernel(split_ptr(P.km, SK_SPLIT0), dim3(P.split0_grid), dim3(FUSED_THREADS), args,
+                           split_smem(P.nb, SK_SPLIT0), st) != cudaSuccess)
         s = DRTOPK_ECUDA;
     }
     if (s == DRTOPK_OK) {

@@ -40,6 +40,7 @@ struct EngineCfg {
   int max_levels;      // stop after this many levels
   int thr_only;        // only the final range is wanted (histogram passes, no appends)
   int key_from_payload;  // key = ~payload (fill by lowest payload)
+  int skip_split0;     // level 0's split (top list, next set, level-1 histogram) was made by another kernel
 };
 
 struct RunBufs {
@@ -52,6 +53,11 @@ struct RunBufs {
   uint64_t top_cap;     // entries the top list holds
   uint64_t cbuf_cap;    // entries each compact buffer holds
   uint32_t* err;        // error word: DE_OVERFLOW when an append would pass a capacity
+  // caller's output (value bits / index, either may be null): a split made
+  // with DIRECT output writes its top entries there instead of rb.top
+  int out_km;
+  uint32_t* out_vals;
+  int64_t* out_idx;
 };
 
 struct Level {
@@ -210,12 +216,57 @@ DRTOPK_DEV uint32_t src_key1(const Src& s, uint64_t i) {
   return s.raw_input ? to_key<KM>(v) : v;
 }
 
-// entry visitor over the source set: tiles of blockDim*16 entries per block
-// (16 independent coalesced loads in flight per thread), trip count uniform
-// per block.  fn(key, payload, valid) is called for every slot; valid=false
-// for padding.  Used by histogram passes (no appends inside fn).
+// entry visitor over the source set, for histogram passes (no appends inside
+// fn).  fn(key, payload, valid) may be called by a subset of a warp's lanes:
+// warp-collective work inside it must use __activemask().  A 16-byte
+// aligned source is read as 16-byte words (4 keys or 2 pairs), FOR_EACH_V
+// per thread in flight; the < 4-entry remainder is visited by the team's
+// first CTA.  Otherwise tiles of blockDim*16 entries with one 4- or 8-byte
+// load each.
+constexpr int FOR_EACH_V = 4;
+
 template <int KM, typename F>
 DRTOPK_DEV void for_each_src(const Team& tm, const Src& s, bool from_pairs, uint64_t count, F&& fn) {
+  const uint32_t* base = from_pairs ? reinterpret_cast<const uint32_t*>(s.pairs) : s.keys;
+  if ((reinterpret_cast<uintptr_t>(base) & 15u) == 0) {
+    const int per = from_pairs ? 2 : 4;  // entries per 16-byte word
+    const uint64_t nw = count / (uint64_t)per;
+    const uint64_t T = (uint64_t)blockDim.x * FOR_EACH_V;
+    for (uint64_t tb = (uint64_t)tm.rank * T; tb < nw; tb += (uint64_t)tm.size * T) {
+      uint4 w[FOR_EACH_V];
+#pragma unroll
+      for (int v = 0; v < FOR_EACH_V; ++v) {
+        const uint64_t q = tb + (uint64_t)v * blockDim.x + threadIdx.x;
+        w[v] = q < nw ? ld_cg_v4(base + 4 * q) : make_uint4(0u, 0u, 0u, 0u);
+      }
+#pragma unroll
+      for (int v = 0; v < FOR_EACH_V; ++v) {
+        const uint64_t q = tb + (uint64_t)v * blockDim.x + threadIdx.x;
+        const bool valid = q < nw;
+        if (from_pairs) {
+          fn(w[v].x, w[v].y, valid);
+          fn(w[v].z, w[v].w, valid);
+        } else {
+          const uint32_t i0 = (uint32_t)(4 * q);
+          const bool raw = s.raw_input;
+          fn(raw ? to_key<KM>(w[v].x) : w[v].x, i0, valid);
+          fn(raw ? to_key<KM>(w[v].y) : w[v].y, i0 + 1, valid);
+          fn(raw ? to_key<KM>(w[v].z) : w[v].z, i0 + 2, valid);
+          fn(raw ? to_key<KM>(w[v].w) : w[v].w, i0 + 3, valid);
+        }
+      }
+    }
+    const uint64_t i = nw * (uint64_t)per + threadIdx.x;
+    if (tm.rank == 0 && i < count) {
+      if (from_pairs) {
+        const uint2 x = ld_cg_v2(reinterpret_cast<const uint32_t*>(s.pairs + i));
+        fn(x.x, x.y, true);
+      } else {
+        fn(src_key1<KM>(s, i), (uint32_t)i, true);
+      }
+    }
+    return;
+  }
   constexpr int E = 16;
   const uint64_t T = (uint64_t)blockDim.x * E;
   for (uint64_t tb = (uint64_t)tm.rank * T; tb < count; tb += (uint64_t)tm.size * T) {
@@ -245,10 +296,12 @@ constexpr int SPLIT_E = 16;  // entries per thread per tile
 
 // One level's split of a set: keys above N's range -> top list, keys inside
 // -> next set (+ histogram of the next level).  Tiles of blockDim*SPLIT_E
-// entries, coalesced loads, one block-aggregated append per tile.
-template <int KM>
+// entries, coalesced loads, one block-aggregated append per tile.  Slots are
+// numbered warp by warp and entry by entry (ballot ranks), so the lanes of a
+// warp write consecutive slots: the appends leave as coalesced stores.
+template <int KM, bool DIRECT = false, int SPLIT_E = drtopk::SPLIT_E>
 DRTOPK_DEV void split_tiles(const Team& tm, const EngineCfg& c, const Src& s, bool pairs, uint64_t count,
-                            const Level& N, bool want_hist, uint2* top, uint32_t* top_count, uint2* nxt,
+                            const Level& N, bool want_hist, const RunBufs& ob, uint32_t* top_count, uint2* nxt,
                             uint32_t* nxt_count, uint32_t* s_hist, uint64_t top_cap, uint64_t nxt_cap,
                             uint32_t* err) {
   const uint64_t T = (uint64_t)blockDim.x * SPLIT_E;
@@ -282,23 +335,41 @@ DRTOPK_DEV void split_tiles(const Team& tm, const EngineCfg& c, const Src& s, bo
       ca += u;
       cb += w;
     }
-    Slots2 sl = block_append2(ca, cb, top_count, nxt_count);
+    // warp totals go in through lane 0; every lane then starts from the
+    // warp's base
+    const unsigned lane = threadIdx.x & 31u;
+    const uint32_t wa = __reduce_add_sync(0xffffffffu, ca), wb = __reduce_add_sync(0xffffffffu, cb);
+    Slots2 sl = block_append2(lane == 0 ? wa : 0u, lane == 0 ? wb : 0u, top_count, nxt_count);
+    sl.a = __shfl_sync(0xffffffffu, sl.a, 0);
+    sl.b = __shfl_sync(0xffffffffu, sl.b, 0);
+    const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
     for (int e = 0; e < SPLIT_E; ++e) {
       // the histogram bounds both counts; a capacity check still guards
       // every address computed from device data
-      if ((up >> e) & 1u) {
-        if (sl.a < top_cap) top[sl.a] = make_uint2(val[e], pay[e]);
+      const bool ue = (up >> e) & 1u, ie = (in >> e) & 1u;
+      const unsigned mu = __ballot_sync(0xffffffffu, ue), mi = __ballot_sync(0xffffffffu, ie);
+      if (ue) {
+        const uint32_t slot = sl.a + __popc(mu & lt);
+        if (slot < top_cap) {
+          if (DIRECT) {
+            if (ob.out_vals) ob.out_vals[slot] = from_key(val[e], ob.out_km);
+            if (ob.out_idx) ob.out_idx[slot] = (int64_t)pay[e];
+          } else {
+            ob.top[slot] = make_uint2(val[e], pay[e]);
+          }
+        }
         else ovf = true;
-        ++sl.a;
       }
-      if ((in >> e) & 1u) {
-        if (sl.b < nxt_cap) nxt[sl.b] = make_uint2(val[e], pay[e]);
+      if (ie) {
+        const uint32_t slot = sl.b + __popc(mi & lt);
+        if (slot < nxt_cap) nxt[slot] = make_uint2(val[e], pay[e]);
         else ovf = true;
-        ++sl.b;
         const uint32_t key = c.key_from_payload ? ~pay[e] : val[e];
         if (want_hist) hist_add_warp(s_hist, bin_of(key, N.lo, N.w, N.wshift));
       }
+      sl.a += __popc(mu);
+      sl.b += __popc(mi);
     }
   }
   if (ovf && err) atomicOr(err, (uint32_t)DE_OVERFLOW);
@@ -349,9 +420,11 @@ DRTOPK_DEV int run_levels(const EngineCfg& c, const Src& src0, bool src0_pairs, 
       s.pairs = rb.cbuf[(j - 1) & 1];
       cnt = ld_cg_u32(rb.set_count + j);
     }
-    split_tiles<KM>(tm, c, s, from_pairs, cnt, N, want_hist, rb.top, rb.top_count, rb.cbuf[j & 1],
-                    rb.set_count + j + 1, s_hist, rb.top_cap, rb.cbuf_cap, rb.err);
-    if (want_hist) flush_hist(s_hist, Hn, c.nb);
+    if (!(c.skip_split0 && j == 0)) {
+      split_tiles<KM>(tm, c, s, from_pairs, cnt, N, want_hist, rb, rb.top_count, rb.cbuf[j & 1],
+                      rb.set_count + j + 1, s_hist, rb.top_cap, rb.cbuf_cap, rb.err);
+      if (want_hist) flush_hist(s_hist, Hn, c.nb);
+    }
     if (!team_sync(tm)) { ok = false; break; }
     L = N;
     if (done) {
@@ -645,6 +718,24 @@ DRTOPK_DEV Level radix_level0(int nbits, uint32_t R) {
   return L;
 }
 
+// Level 0 of a second select whose candidates are all >= thr: the range
+// [thr, 2^32) in nb = 2^nbits bins of the narrowest power-of-two width that
+// covers it (thr = 0 gives radix_level0).  Later levels take nbits off the
+// width as usual.  The exact k-th and the top list do not depend on where
+// the digit boundaries lie; anchoring them at thr spreads the candidates
+// over all bins instead of the few top digits above thr.
+DRTOPK_DEV int cand_shift(uint32_t thr, int nbits) {
+  const uint32_t top = 0xffffffffu - thr;  // largest key - thr
+  const int bits = 32 - __clz(top);
+  return max(0, bits - nbits);
+}
+
+DRTOPK_DEV Level cand_level0(uint32_t thr, int nbits, uint32_t R) {
+  Level L;
+  L.lo = thr; L.hi = 0xffffffffu; L.wshift = cand_shift(thr, nbits); L.w = 1u << L.wshift; L.R = R;
+  return L;
+}
+
 DRTOPK_DEV Level bucket_level0(uint32_t mn, uint32_t mx, int nb, uint32_t R) {
   Level L;
   L.lo = mn; L.hi = mx; L.wshift = -1;
@@ -671,7 +762,7 @@ DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_p
     res.levels = (int)ld_cg_u32(rb.res + 2);
     res.ok = ld_cg_u32(rb.res + 3) ? 1 : 0;
   };
-  if (can_small) {
+  if (can_small && !c.skip_split0) {
     const uint64_t n0 = src0_pairs ? (uint64_t)ld_cg_u32(src0.count_dev) : src0.count;
     if (n0 <= (uint64_t)SMALL_SET) {
       finish_small(src0, src0_pairs, (uint32_t)n0, L0, 0);
@@ -742,7 +833,8 @@ DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_p
   if (tm.rank == 0 && threadIdx.x == 0) {
     uint2 e = ld_cg_v2(reinterpret_cast<const uint32_t*>(fr.cbuf[eqb2]));
     uint32_t slot = atomicAdd(rb.top_count, 1u);
-    rb.top[slot] = e;
+    if (slot < rb.top_cap) rb.top[slot] = e;
+    else if (rb.err) atomicOr(rb.err, (uint32_t)DE_OVERFLOW);
   }
   if (!team_sync(tm)) res.ok = 0;
   return res;

@@ -16,8 +16,8 @@
 //            optimized 1574-1607); beta: FindTopKRanges_beta 560-598 (Max and
 //            Second >= thr -> whole subrange; Max only -> that one key) fused
 //            with CreateConcatenateRange_Beta_optimized 1609-1639.  Appends
-//            are warp-aggregated; the same pass histograms the candidates'
-//            top digit (first level of phase 3).
+//            are block-aggregated; the same pass histograms the candidates
+//            over the first level of phase 3, which spans [threshold, 2^32).
 //   phase 3  second select over the candidates (radix_select_inplace
 //            1410-1470): exact k-th largest, plus the top-k list with ties
 //            broken by lowest index.
@@ -68,6 +68,9 @@ struct FusedArgs {
   uint32_t* thr_word;     // threshold handed between launches in split mode
   uint32_t* tail_flag;    // shared-memory tail: 1 done, 2 fall back to the general path
   int phase_lo, phase_hi; // phases run by this launch of k_fused (1..3)
+  int first_pre;          // split mode: the first select runs in k_level_hist / k_filter
+  int split0;             // split mode: level 0 of the second select runs in k_split0
+  int direct0;            // ... writing its top entries straight to the (unsorted) output
   GridBar gb;
 };
 
@@ -77,18 +80,6 @@ enum StatSlot : int {
 };
 
 // --------------------------------------------------------------- gathers
-template <int KM>
-DRTOPK_DEV void emit_candidate(const FusedArgs& a, bool take, uint32_t key, uint32_t idx, uint32_t* s_hist,
-                               uint32_t& mlo, uint32_t& mhi, bool& ovf) {
-  uint32_t slot = warp_append(take, a.cand_count);
-  if (take) {
-    if (slot < a.cand_cap) a.cand[slot] = make_uint2(key, idx);
-    else ovf = true;
-    if (a.bucket) { mlo = max(mlo, ~key); mhi = max(mhi, key); }
-    else hist_add_warp(s_hist, key >> (32 - a.nbits));
-  }
-}
-
 template <int KM>
 DRTOPK_DEV void load4(const FusedArgs& a, uint64_t base, bool vec, uint32_t (&v)[4]) {
   if (vec) {
@@ -115,6 +106,7 @@ DRTOPK_DEV void gather_list(const Team& tm, const FusedArgs& a, const uint2* ids
   const int gk = 1 << gshift;
   const uint64_t units = (nsub * S) >> gshift;
   const uint64_t T = (uint64_t)blockDim.x * GATHER_U;
+  const int cs = cand_shift(thr, a.nbits);
   for (uint64_t tb = (uint64_t)tm.rank * T; tb < units; tb += (uint64_t)tm.size * T) {
     uint32_t v[GATHER_U][4];
     uint32_t base[GATHER_U];  // key index of the granule (n < 2^32)
@@ -160,7 +152,7 @@ DRTOPK_DEV void gather_list(const Team& tm, const FusedArgs& a, const uint2* ids
           else ovf = true;
           ++slot;
           if (a.bucket) { mlo = max(mlo, ~key); mhi = max(mhi, key); }
-          else hist_add_warp(s_hist, key >> (32 - a.nbits));
+          else hist_add_warp(s_hist, (key - thr) >> cs);
         }
       }
   }
@@ -175,6 +167,7 @@ template <int KM>
 DRTOPK_DEV void filter_beta(const Team& tm, const FusedArgs& a, uint32_t thr, uint32_t* s_hist, uint32_t& mlo,
                             uint32_t& mhi, bool& ovf) {
   const uint64_t T = (uint64_t)blockDim.x * FILTER_E;
+  const int hsh = cand_shift(thr, a.nbits);
   for (uint64_t tb = (uint64_t)tm.rank * T; tb < a.M; tb += (uint64_t)tm.size * T) {
     uint32_t m1[FILTER_E];
     uint32_t lon = 0, sel = 0, cl = 0, cs = 0;
@@ -204,7 +197,7 @@ DRTOPK_DEV void filter_beta(const Team& tm, const FusedArgs& a, uint32_t thr, ui
         else ovf = true;
         ++sl.a;
         if (a.bucket) { mlo = max(mlo, ~m1[q]); mhi = max(mhi, m1[q]); }
-        else hist_add_warp(s_hist, m1[q] >> (32 - a.nbits));
+        else hist_add_warp(s_hist, (m1[q] - thr) >> hsh);
       }
       if ((sel >> q) & 1u) a.sel[sl.b++] = (uint32_t)j;
     }
@@ -373,7 +366,7 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
   const int D = 32 / a.nbits;
   uint32_t thr1 = 0, nsel = 0, nlonely = 0;
   int lvA = 0;
-  if (lead) stamp(a.stats, 16);
+  if (lead && a.phase_lo <= 1) stamp(a.stats, 16);
 
   // ---------------- phase 1: first select on the delegates
   if (a.phase_lo > 1) {
@@ -499,11 +492,15 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
     hist_pass<KM>(tm, sc, pairs, false, L0c, a.nb, a.C.H[0], s_hist);
     if (!team_sync(tm)) return;
   } else {
-    L0c = radix_level0(a.nbits, a.k);
+    // candidates of the sampled paths are all >= thr1 (their level-0
+    // histogram was built against this level by the concatenation)
+    L0c = a.path == PATH_PLAIN ? radix_level0(a.nbits, a.k) : cand_level0(thr1, a.nbits, a.k);
   }
   EngineCfg cc;
   cc.bucket = a.bucket; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
-  cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0;
+  cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0; cc.skip_split0 = a.split0;
+  // entries k_split0 already wrote to the output (slots [0, c0) of the list)
+  const uint32_t c0 = a.direct0 ? ld_cg_u32(a.C.top_count) : 0u;
   RunResult rc = run_select<KM>(cc, sc, pairs, a.C, a.CF, L0c, s_hist, tm, s_fast);
   if (!rc.ok) { if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL); return; }
   const uint32_t K = rc.kth;
@@ -529,10 +526,11 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
   const uint64_t g = (uint64_t)tm.rank * blockDim.x + threadIdx.x;
   const uint64_t G = (uint64_t)tm.size * blockDim.x;
   if (!a.sorted) {
-    team_load_loop<8>(tm, a.k, [&](uint64_t i) { return ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + i)); },
+    team_load_loop<8>(tm, a.k - c0,
+                      [&](uint64_t i) { return ld_cg_v2(reinterpret_cast<const uint32_t*>(a.C.top + c0 + i)); },
                       [&](uint64_t i, uint2 e) {
-                        if (a.out_vals) a.out_vals[i] = from_key(e.x, a.km);
-                        if (a.out_idx) a.out_idx[i] = (int64_t)e.y;
+                        if (a.out_vals) a.out_vals[c0 + i] = from_key(e.x, a.km);
+                        if (a.out_idx) a.out_idx[c0 + i] = (int64_t)e.y;
                       });
     return;
   }
@@ -596,6 +594,74 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused_cl(FusedArgs a0, const 
 // (many more resident warps than the cooperative kernel) between two
 // launches of k_fused (phase 1, then phase 3).  The threshold comes from
 // a.thr_word; counts are read after the kernel boundary.
+//
+// Both kernels work warp by warp with no block barrier in the loop: a warp
+// compacts what it keeps into its own stage in shared memory (one warp scan
+// per round) and drains the stage to global memory in runs of up to
+// SPLIT_STAGE entries with one atomic per run, so appends neither contend on
+// the global counters nor stall the warp.  The second select's level-0
+// histogram is taken from the stage as it drains.
+constexpr int SPLIT_STAGE = 512;                 // staged entries per warp (k_filter)
+constexpr int SPLIT_WARPS = FUSED_THREADS / 32;
+constexpr int FILTER_Q = 8;                      // subranges per lane per batch (k_filter)
+constexpr int GATHER_R = 4;                      // granules per lane per round (k_gather)
+constexpr int GATHER_STAGE = 32 * 4 * GATHER_R;  // staged candidates per warp (k_gather): one round's worth
+// shared memory of the split kernels after the histogram words
+constexpr size_t SPLIT_FILTER_SMEM = (size_t)SPLIT_WARPS * SPLIT_STAGE * 12;  // candidate + selected-id stages
+constexpr size_t SPLIT_GATHER_SMEM = (size_t)SPLIT_WARPS * GATHER_STAGE * 8;
+
+DRTOPK_DEV int split_hist_words(int nb) { return (max(nb, 256) + 3) & ~3; }
+
+// exclusive prefix of v over the warp; total in *tot
+DRTOPK_DEV uint32_t warp_excl_scan(uint32_t v, uint32_t& tot) {
+  const unsigned lane = lane_id();
+  uint32_t x = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+    if ((int)lane >= off) x += y;
+  }
+  tot = __shfl_sync(0xffffffffu, x, 31);
+  return x - v;
+}
+
+// A warp's stage of (key, index) candidates.  Every member is warp-uniform
+// except the stage contents; all calls are made by the full warp.
+struct CandStage {
+  uint2* buf;
+  uint32_t cap;
+  uint32_t n;
+  uint32_t thr;
+  int cs;
+  uint32_t mlo, mhi;
+  bool ovf;
+
+  DRTOPK_DEV void drain(const FusedArgs& a, uint32_t* s_hist) {
+    __syncwarp();
+    const unsigned lane = lane_id();
+    if (n == 0) return;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(a.cand_count, n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t i = lane; i < n; i += 32) {
+      const uint2 v = buf[i];
+      if ((uint64_t)base + i < a.cand_cap) a.cand[base + i] = v;
+      else ovf = true;
+      if (a.bucket) { mlo = max(mlo, ~v.x); mhi = max(mhi, v.x); }
+      else hist_add_warp(s_hist, (v.x - thr) >> cs);
+    }
+    __syncwarp();
+    n = 0;
+  }
+  // room for `tot` more entries (tot <= cap); returns the first slot
+  DRTOPK_DEV uint32_t reserve(const FusedArgs& a, uint32_t* s_hist, uint32_t tot) {
+    if (n + tot > cap) drain(a, s_hist);
+    const uint32_t at = n;
+    n += tot;
+    return at;
+  }
+};
+
 DRTOPK_DEV void flush_cand_stats(const FusedArgs& a, uint32_t* s_hist, uint32_t mlo, uint32_t mhi) {
   if (a.bucket) {
 #pragma unroll
@@ -609,48 +675,317 @@ DRTOPK_DEV void flush_cand_stats(const FusedArgs& a, uint32_t* s_hist, uint32_t 
   }
 }
 
+// Convergent histogram increment (all 32 lanes call it; `in` selects the
+// lanes that count): one atomic when every counting lane hits the same bin.
+DRTOPK_DEV void hist_add_conv(uint32_t* h, bool in, uint32_t bin) {
+  const unsigned m = __ballot_sync(0xffffffffu, in);
+  if (m == 0u) return;
+  const int leader = __ffs(m) - 1;
+  const uint32_t b0 = __shfl_sync(0xffffffffu, bin, leader);
+  if (__ballot_sync(0xffffffffu, in && bin == b0) == m) {
+    if ((int)lane_id() == leader) atomicAdd(&h[b0], (uint32_t)__popc(m));
+  } else if (in) {
+    atomicAdd(&h[bin], 1u);
+  }
+}
+
+// First select of the beta path in split mode (radix, first_levels <= 2):
+// the threshold-only picks of radix_select_inplace_firsttopk_beta
+// (radixselect.cuh:1727-1780) -- the same picks run_levels makes -- from
+// the delegate histograms A.H[0] (sampler) and A.H[1] (k_level_hist).  Every
+// CTA computes them redundantly; `upto` levels are picked.
+DRTOPK_DEV Level beta_first_levels(const FusedArgs& a, int upto, int& levels) {
+  EngineCfg c;
+  c.bucket = 0; c.nbits = a.nbits; c.nb = a.nb; c.stop_single = 0; c.thr_only = 1;
+  c.max_levels = a.first_levels; c.key_from_payload = 0;
+  Level L = radix_level0(a.nbits, a.k);
+  levels = 0;
+  for (int j = 0; j < upto; ++j) {
+    const Pick p = block_pick<false>(a.A.H[j], a.nb, L.R);
+    Level N;
+    const bool done = advance(c, L, p, j, N);
+    L = N;
+    levels = j + 1;
+    if (done) break;
+  }
+  return L;
+}
+
+// Level-1 histogram of the delegates for the split-mode first select: every
+// CTA picks the level-0 bin, then the delegates inside it are counted over
+// the next digit into A.H[1] (16-byte loads, LEVEL_HIST_V per thread in flight).
+constexpr int LEVEL_HIST_V = 8;
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_level_hist(FusedArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  uint32_t* s_hist = s_dyn;
+  if (blockIdx.x == 0 && threadIdx.x == 0) stamp(a.stats, 16);
+  clear_hist(s_hist, a.nb);
+  int lv = 0;
+  const Level N = beta_first_levels(a, 1, lv);
+  const uint64_t nkeys = 2 * a.M;
+  const uint64_t nw = nkeys / 4;
+  const uint64_t T = (uint64_t)blockDim.x * LEVEL_HIST_V;
+  for (uint64_t tb = (uint64_t)blockIdx.x * T; tb < nw; tb += (uint64_t)gridDim.x * T) {
+    uint4 w[LEVEL_HIST_V];
+#pragma unroll
+    for (int v = 0; v < LEVEL_HIST_V; ++v) {
+      const uint64_t q = tb + (uint64_t)v * blockDim.x + threadIdx.x;
+      w[v] = q < nw ? __ldg(reinterpret_cast<const uint4*>(a.del) + q) : make_uint4(0u, 0u, 0u, 0u);
+    }
+#pragma unroll
+    for (int v = 0; v < LEVEL_HIST_V; ++v) {
+      const bool valid = tb + (uint64_t)v * blockDim.x + threadIdx.x < nw;
+      const uint32_t kk[4] = {w[v].x, w[v].y, w[v].z, w[v].w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const bool in = valid && kk[e] >= N.lo && kk[e] <= N.hi;
+        hist_add_conv(s_hist, in, in ? bin_of(kk[e], N.lo, N.w, N.wshift) : 0u);
+      }
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x < nkeys - nw * 4) {
+    const uint32_t key = __ldg(a.del + nw * 4 + threadIdx.x);
+    if (key >= N.lo && key <= N.hi) atomicAdd(&s_hist[bin_of(key, N.lo, N.w, N.wshift)], 1u);
+  }
+  flush_hist(s_hist, a.A.H[1], a.nb);
+}
+
+// Level 0 of the second select (radix_select_inplace 1410-1470) over a large
+// candidate set, as an ordinary kernel: every CTA makes the level-0 pick
+// from C.H[0] (the concatenation's histogram) -- the pick the cooperative
+// kernel then makes again -- and splits the candidates: above the chosen
+// bin -> the top list, or straight to the output when it is unsorted
+// (direct0); inside it -> the next set, with the level-1 histogram.
+constexpr int SPLIT0_E = 8;  // entries per thread per tile (register budget of 4 CTAs / SM)
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_split0(FusedArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  uint32_t* s_hist = s_dyn;
+  const uint32_t thr = ld_cg_u32(a.thr_word);
+  const uint32_t ncand = ld_cg_u32(a.cand_count);
+  if (ncand < a.k || ncand > a.cand_cap) return;  // uniform; the second select reports it
+  EngineCfg cc;
+  cc.bucket = 0; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
+  cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0; cc.skip_split0 = 0;
+  const Level L0 = cand_level0(thr, a.nbits, a.k);
+  const Pick p = block_pick<false>(a.C.H[0], a.nb, L0.R);
+  Level N;
+  const bool done = advance(cc, L0, p, 0, N);
+  clear_hist(s_hist, a.nb);
+  Src sc = {};
+  sc.pairs = a.cand;
+  sc.count_dev = a.cand_count;
+  const Team tm = grid_team(a.gb);
+  if (a.direct0)
+    split_tiles<KM, true, SPLIT0_E>(tm, cc, sc, true, ncand, N, !done, a.C, a.C.top_count, a.C.cbuf[0], a.C.set_count + 1,
+                          s_hist, a.C.top_cap, a.C.cbuf_cap, a.C.err);
+  else
+    split_tiles<KM, false, SPLIT0_E>(tm, cc, sc, true, ncand, N, !done, a.C, a.C.top_count, a.C.cbuf[0], a.C.set_count + 1,
+                           s_hist, a.C.top_cap, a.C.cbuf_cap, a.C.err);
+  if (!done) flush_hist(s_hist, a.C.H[1], a.nb);
+}
+
+// Beta filter (FindTopKRanges_beta, radixselect.cuh:560-598) over batches of
+// 32*FILTER_Q subranges per warp: Max and Second >= thr -> subrange id to
+// the selected list; Max >= thr only -> Max is a candidate, at its position.
 template <int KM>
 __global__ void __launch_bounds__(FUSED_THREADS) k_filter(FusedArgs a) {
   extern __shared__ __align__(16) uint32_t s_dyn[];
   uint32_t* s_hist = s_dyn;
-  const uint32_t thr = ld_cg_u32(a.thr_word);
+  const int hw = split_hist_words(a.nb);
+  const unsigned lane = lane_id();
+  const int wib = threadIdx.x >> 5;
+  uint2* cstage = reinterpret_cast<uint2*>(s_dyn + hw) + (size_t)wib * SPLIT_STAGE;
+  uint32_t* sstage = reinterpret_cast<uint32_t*>(reinterpret_cast<uint2*>(s_dyn + hw) + (size_t)SPLIT_WARPS * SPLIT_STAGE) +
+                     (size_t)wib * SPLIT_STAGE;
+  uint32_t thr;
+  if (a.first_pre) {
+    // the first select ends here: every CTA picks the threshold itself
+    int lv = 0;
+    thr = a.first_levels > 0 ? beta_first_levels(a, a.first_levels, lv).lo : 0u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      *a.thr_word = thr;
+      a.stats[ST_LVA] = (uint32_t)lv;
+      if (a.first_levels < 2) stamp(a.stats, 16);
+      stamp(a.stats, 18);
+    }
+  } else {
+    thr = ld_cg_u32(a.thr_word);
+  }
   clear_hist(s_hist, a.nb);
-  uint32_t mlo = 0, mhi = 0;
-  bool ovf = false;
-  filter_beta<KM>(grid_team(a.gb), a, thr, s_hist, mlo, mhi, ovf);
-  if (ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
-  flush_cand_stats(a, s_hist, mlo, mhi);
+  CandStage cst = {cstage, (uint32_t)SPLIT_STAGE, 0u, thr, cand_shift(thr, a.nbits), 0u, 0u, false};
+  uint32_t ns = 0;               // staged selected ids (warp-uniform)
+  uint32_t nsel = 0, nlone = 0;  // this warp's totals
+  auto drain_sel = [&]() {
+    __syncwarp();
+    if (ns == 0) return;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(a.sel_count, ns);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t i = lane; i < ns; i += 32)
+      if ((uint64_t)base + i < a.M) a.sel[base + i] = sstage[i];
+      else cst.ovf = true;
+    __syncwarp();
+    ns = 0;
+  };
+  const uint64_t B = 32ull * FILTER_Q;
+  const uint64_t nbatch = (a.M + B - 1) / B;
+  const uint64_t gw = (uint64_t)blockIdx.x * SPLIT_WARPS + wib, nw = (uint64_t)gridDim.x * SPLIT_WARPS;
+  const uint2* del2 = reinterpret_cast<const uint2*>(a.del);
+  for (uint64_t bt = gw; bt < nbatch; bt += nw) {
+    const uint64_t j0 = bt * B;
+    uint2 d[FILTER_Q];
+    uint32_t ps[FILTER_Q];
+#pragma unroll
+    for (int q = 0; q < FILTER_Q; ++q) {
+      const uint64_t j = j0 + (uint64_t)q * 32 + lane;
+      d[q] = j < a.M ? __ldg(del2 + j) : make_uint2(0u, 0u);
+      ps[q] = (a.has_pos && j < a.M) ? (uint32_t)__ldg(a.pos + j) : 0u;
+    }
+    uint32_t lone = 0, sel = 0;
+#pragma unroll
+    for (int q = 0; q < FILTER_Q; ++q) {
+      const uint64_t j = j0 + (uint64_t)q * 32 + lane;
+      const bool v = j < a.M && d[q].x >= thr;
+      sel |= (uint32_t)(v && d[q].y >= thr) << q;
+      lone |= (uint32_t)(v && d[q].y < thr) << q;
+    }
+    uint32_t tl = 0, ts = 0;
+    const uint32_t ol = warp_excl_scan(__popc(lone), tl);
+    const uint32_t os = warp_excl_scan(__popc(sel), ts);
+    nlone += tl;
+    nsel += ts;
+    if (tl) {
+      uint32_t at = cst.reserve(a, s_hist, tl) + ol;
+#pragma unroll
+      for (int q = 0; q < FILTER_Q; ++q)
+        if ((lone >> q) & 1u) {
+          const uint64_t j = j0 + (uint64_t)q * 32 + lane;
+          cstage[at++] = make_uint2(d[q].x, (uint32_t)(j << a.alpha) + ps[q]);
+        }
+    }
+    if (ts) {
+      if (ns + ts > (uint32_t)SPLIT_STAGE) drain_sel();
+      uint32_t at = ns + os;
+#pragma unroll
+      for (int q = 0; q < FILTER_Q; ++q)
+        if ((sel >> q) & 1u) sstage[at++] = (uint32_t)(j0 + (uint64_t)q * 32 + lane);
+      ns += ts;
+    }
+  }
+  cst.drain(a, s_hist);
+  drain_sel();
+  if (lane == 0 && nlone) atomicAdd(a.stats + ST_NLONELY, nlone);
+  (void)nsel;
+  if (cst.ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
+  flush_cand_stats(a, s_hist, cst.mlo, cst.mhi);
 }
 
+// Keys >= thr of the kept subranges: the default path's k subranges (ids in
+// the .y of the first select's top list) or the beta path's selected list.
+// The virtual space of count*S keys is cut into granules of min(4, S) keys;
+// each warp takes rounds of 32*GATHER_R granules.
 template <int KM>
-__global__ void __launch_bounds__(FUSED_THREADS) k_gather(FusedArgs a) {
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_gather(FusedArgs a) {
   extern __shared__ __align__(16) uint32_t s_dyn[];
   uint32_t* s_hist = s_dyn;
+  const int hw = split_hist_words(a.nb);
+  const unsigned lane = lane_id();
+  const int wib = threadIdx.x >> 5;
+  uint2* cstage = reinterpret_cast<uint2*>(s_dyn + hw) + (size_t)wib * GATHER_STAGE;
   const uint32_t thr = ld_cg_u32(a.thr_word);
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   uint64_t nsub;
+  const uint2* ids2 = nullptr;
+  const uint32_t* ids1 = nullptr;
   if (a.path == PATH_DEFAULT) {
     if (ld_cg_u32(a.A.top_count) != a.k) {  // uniform: written by the previous launch
       if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
       return;
     }
     nsub = a.k;
+    ids2 = a.A.top;
   } else {
     nsub = ld_cg_u32(a.sel_count);
     if (nsub > a.M) {
       if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
       return;
     }
-    if (lead) a.stats[ST_NLONELY] = ld_cg_u32(a.cand_count);  // lonely candidates came first
+    ids1 = a.sel;
   }
   clear_hist(s_hist, a.nb);
-  uint32_t mlo = 0, mhi = 0;
-  bool ovf = false;
-  const Team tm = grid_team(a.gb);
-  if (a.path == PATH_DEFAULT) gather_list<KM, 4>(tm, a, a.A.top, nullptr, nsub, thr, s_hist, mlo, mhi, ovf);
-  else gather_list<KM, 4>(tm, a, nullptr, a.sel, nsub, thr, s_hist, mlo, mhi, ovf);
-  if (ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
-  flush_cand_stats(a, s_hist, mlo, mhi);
+  CandStage cst = {cstage, (uint32_t)GATHER_STAGE, 0u, thr, cand_shift(thr, a.nbits), 0u, 0u, false};
+  const int alpha = a.alpha;
+  const int gsh = alpha >= 2 ? 2 : alpha;  // log2 keys per granule
+  const int gk = 1 << gsh;
+  const int upg = alpha - gsh;             // log2 granules per subrange
+  const uint64_t gmask = (1ull << upg) - 1ull;
+  const uint64_t units = nsub << upg;
+  const uint64_t R = 32ull * GATHER_R;
+  const uint64_t gw = (uint64_t)blockIdx.x * SPLIT_WARPS + wib, nw = (uint64_t)gridDim.x * SPLIT_WARPS;
+  // subrange ids of a round's granules; the next round's ids are loaded while
+  // this round's keys are in flight
+  auto load_ids = [&](uint64_t ub, uint32_t (&sub)[GATHER_R]) {
+#pragma unroll
+    for (int r = 0; r < GATHER_R; ++r) {
+      const uint64_t u = ub + (uint64_t)r * 32 + lane;
+      sub[r] = 0;
+      if (u < units) sub[r] = ids2 ? __ldg(ids2 + (u >> upg)).y : __ldg(ids1 + (u >> upg));
+    }
+  };
+  uint32_t subn[GATHER_R];
+  if (gw * R < units) load_ids(gw * R, subn);
+  for (uint64_t u0 = gw * R; u0 < units; u0 += nw * R) {
+    uint32_t v[GATHER_R][4];
+    uint32_t kb[GATHER_R];
+    uint32_t sub[GATHER_R];
+#pragma unroll
+    for (int r = 0; r < GATHER_R; ++r) sub[r] = subn[r];
+#pragma unroll
+    for (int r = 0; r < GATHER_R; ++r) {
+      const uint64_t u = u0 + (uint64_t)r * 32 + lane;
+      kb[r] = (uint32_t)(((uint64_t)sub[r] << alpha) + ((u & gmask) << gsh));
+      v[r][0] = v[r][1] = v[r][2] = v[r][3] = 0u;
+      if (u < units) {
+        if (gk == 4 && a.vec_ok && (uint64_t)kb[r] + 4 <= a.n) {
+          const uint4 q = __ldg(reinterpret_cast<const uint4*>(a.keys + kb[r]));
+          v[r][0] = q.x; v[r][1] = q.y; v[r][2] = q.z; v[r][3] = q.w;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            if (e < gk && (uint64_t)kb[r] + e < a.n) v[r][e] = __ldg(a.keys + kb[r] + e);
+        }
+      }
+    }
+    if (u0 + nw * R < units) load_ids(u0 + nw * R, subn);
+    uint32_t take = 0;
+#pragma unroll
+    for (int r = 0; r < GATHER_R; ++r) {
+      const uint64_t u = u0 + (uint64_t)r * 32 + lane;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        v[r][e] = to_key<KM>(v[r][e]);
+        const bool t = u < units && e < gk && (uint64_t)kb[r] + e < a.n && v[r][e] >= thr;
+        take |= (uint32_t)t << (r * 4 + e);
+      }
+    }
+    uint32_t tot = 0;
+    const uint32_t off = warp_excl_scan(__popc(take), tot);
+    if (tot) {
+      uint32_t at = cst.reserve(a, s_hist, tot) + off;
+#pragma unroll
+      for (int r = 0; r < GATHER_R; ++r)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if ((take >> (r * 4 + e)) & 1u) cstage[at++] = make_uint2(v[r][e], kb[r] + e);
+    }
+  }
+  cst.drain(a, s_hist);
+  if (cst.ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
+  flush_cand_stats(a, s_hist, cst.mlo, cst.mhi);
 }
 
 }  // namespace drtopk

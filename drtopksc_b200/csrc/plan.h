@@ -40,7 +40,8 @@ struct Plan {
   int split;           // concatenation as separate kernels (large inputs)
   int cluster;         // > 0: phases after the sampler run in one thread-block cluster of this many CTAs
   int tail;            // 1: phases after the sampler run in one CTA with the sets in shared memory
-  int split_grid, filter_grid;
+  int split_grid, filter_grid, hist_grid, split0_grid;
+  int first_pre;       // split mode: first select in k_level_hist / k_filter (beta, radix, <= 2 levels)
   size_t fused_smem;
   size_t run_words;
   int hist_words;

@@ -248,7 +248,7 @@ DRTOPK_DEV bool tail_small(const FusedArgs& a, uint32_t* s_dyn) {
     EngineCfg cc;
     cc.bucket = 0; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
     cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0;
-    Level L = radix_level0(a.nbits, a.k);
+    Level L = cand_level0(thr1, a.nbits, a.k);  // every candidate is >= thr1 (0 on the plain path)
     int j = 0;
     if (!smem_levels(cc, L, j, sA, sB, n, T, &s_ntop, s_hist)) return fail();
     K = (n == 1) ? sA[0].x : L.lo;
