@@ -625,14 +625,15 @@ static drtopk_status_t launch_coop(void* fn, const Plan& P, void* argp, cudaStre
 }
 
 static drtopk_status_t launch_cluster(const Plan& P, const FusedArgs* a, cudaStream_t st) {
+  const int csize = P.cluster;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(P.cluster);
+  cfg.gridDim = dim3(csize);
   cfg.blockDim = dim3(FUSED_THREADS);
   cfg.dynamicSmemBytes = P.fused_smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = P.cluster;
+  attr[0].val.clusterDim.x = csize;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;

@@ -85,8 +85,10 @@ struct RunResult {
 };
 
 DRTOPK_DEV uint32_t bin_of(uint32_t k, uint32_t lo, uint32_t w, int wshift) {
-  uint32_t d = k - lo;
-  return wshift >= 0 ? (d >> wshift) : (d / w);
+  const uint32_t d = k - lo;
+  if (wshift >= 0) return d >> wshift;  // radix levels (and width-1 bins below them)
+  if (w == 1u) return d;
+  return d / w;                         // bucket levels
 }
 
 // --------------------------------------------------------------- block pick
@@ -306,30 +308,33 @@ DRTOPK_DEV void split_tiles(const Team& tm, const EngineCfg& c, const Src& s, bo
                             uint32_t* err) {
   const uint64_t T = (uint64_t)blockDim.x * SPLIT_E;
   bool ovf = false;
+  const uint32_t span = N.hi - N.lo;
   for (uint64_t tb = (uint64_t)tm.rank * T; tb < count; tb += (uint64_t)tm.size * T) {
+    // entry offsets inside the tile are 32-bit; entries >= rem are padding
+    const uint64_t rem = count - tb;
+    const uint2* tp = s.pairs + tb;
     uint32_t val[SPLIT_E], pay[SPLIT_E];
     uint32_t up = 0, in = 0, ca = 0, cb = 0;
 #pragma unroll
     for (int e = 0; e < SPLIT_E; ++e) {
-      const uint64_t i = tb + (uint64_t)e * blockDim.x + threadIdx.x;
+      const uint32_t o = (uint32_t)e * blockDim.x + threadIdx.x;
       val[e] = 0; pay[e] = 0;
-      if (i < count) {
+      if (o < rem) {
         if (pairs) {
-          uint2 x = ld_cg_v2(reinterpret_cast<const uint32_t*>(s.pairs + i));
+          uint2 x = ld_cg_v2(reinterpret_cast<const uint32_t*>(tp + o));
           val[e] = x.x; pay[e] = x.y;
         } else {
-          val[e] = src_key1<KM>(s, i);
-          pay[e] = (uint32_t)i;
+          val[e] = src_key1<KM>(s, tb + o);
+          pay[e] = (uint32_t)(tb + o);
         }
       }
     }
 #pragma unroll
     for (int e = 0; e < SPLIT_E; ++e) {
-      const uint64_t i = tb + (uint64_t)e * blockDim.x + threadIdx.x;
       const uint32_t key = c.key_from_payload ? ~pay[e] : val[e];
-      const bool valid = i < count;
+      const bool valid = (uint32_t)e * blockDim.x + threadIdx.x < rem;
       const bool u = valid && key > N.hi;
-      const bool w = valid && key >= N.lo && key <= N.hi;
+      const bool w = valid && key - N.lo <= span;
       up |= (uint32_t)u << e;
       in |= (uint32_t)w << e;
       ca += u;

@@ -724,6 +724,8 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_level_hist(FusedArgs a) {
   clear_hist(s_hist, a.nb);
   int lv = 0;
   const Level N = beta_first_levels(a, 1, lv);
+  const uint32_t span = N.hi - N.lo;
+  const int sh = max(N.wshift, 0);  // radix: bins are power-of-two wide (width 1 below the last digit)
   const uint64_t nkeys = 2 * a.M;
   const uint64_t nw = nkeys / 4;
   const uint64_t T = (uint64_t)blockDim.x * LEVEL_HIST_V;
@@ -740,14 +742,18 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_level_hist(FusedArgs a) {
       const uint32_t kk[4] = {w[v].x, w[v].y, w[v].z, w[v].w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        const bool in = valid && kk[e] >= N.lo && kk[e] <= N.hi;
-        hist_add_conv(s_hist, in, in ? bin_of(kk[e], N.lo, N.w, N.wshift) : 0u);
+        const uint32_t d = kk[e] - N.lo;
+        const bool in = valid && d <= span;
+        // plain shared atomics unless at least half the warp counts (then
+        // one atomic when they all share a bin: crowded keys)
+        if (__popc(__ballot_sync(0xffffffffu, in)) >= 16) hist_add_conv(s_hist, in, d >> sh);
+        else if (in) atomicAdd(&s_hist[d >> sh], 1u);
       }
     }
   }
   if (blockIdx.x == 0 && threadIdx.x < nkeys - nw * 4) {
-    const uint32_t key = __ldg(a.del + nw * 4 + threadIdx.x);
-    if (key >= N.lo && key <= N.hi) atomicAdd(&s_hist[bin_of(key, N.lo, N.w, N.wshift)], 1u);
+    const uint32_t d = __ldg(a.del + nw * 4 + threadIdx.x) - N.lo;
+    if (d <= span) atomicAdd(&s_hist[d >> sh], 1u);
   }
   flush_hist(s_hist, a.A.H[1], a.nb);
 }
@@ -835,21 +841,22 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_filter(FusedArgs a) {
   const uint64_t nbatch = (a.M + B - 1) / B;
   const uint64_t gw = (uint64_t)blockIdx.x * SPLIT_WARPS + wib, nw = (uint64_t)gridDim.x * SPLIT_WARPS;
   const uint2* del2 = reinterpret_cast<const uint2*>(a.del);
+  // subrange ids fit 32 bits (M <= n < 2^32); only the batch counter is 64-bit
   for (uint64_t bt = gw; bt < nbatch; bt += nw) {
-    const uint64_t j0 = bt * B;
+    const uint64_t rem = a.M - bt * B;  // > 0
+    const uint32_t j0 = (uint32_t)(bt * B);
     uint2 d[FILTER_Q];
     uint32_t ps[FILTER_Q];
 #pragma unroll
     for (int q = 0; q < FILTER_Q; ++q) {
-      const uint64_t j = j0 + (uint64_t)q * 32 + lane;
-      d[q] = j < a.M ? __ldg(del2 + j) : make_uint2(0u, 0u);
-      ps[q] = (a.has_pos && j < a.M) ? (uint32_t)__ldg(a.pos + j) : 0u;
+      const uint32_t o = (uint32_t)q * 32u + lane;
+      d[q] = o < rem ? __ldg(del2 + j0 + o) : make_uint2(0u, 0u);
+      ps[q] = (a.has_pos && o < rem) ? (uint32_t)__ldg(a.pos + j0 + o) : 0u;
     }
     uint32_t lone = 0, sel = 0;
 #pragma unroll
     for (int q = 0; q < FILTER_Q; ++q) {
-      const uint64_t j = j0 + (uint64_t)q * 32 + lane;
-      const bool v = j < a.M && d[q].x >= thr;
+      const bool v = (uint32_t)q * 32u + lane < rem && d[q].x >= thr;
       sel |= (uint32_t)(v && d[q].y >= thr) << q;
       lone |= (uint32_t)(v && d[q].y < thr) << q;
     }
@@ -860,19 +867,21 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_filter(FusedArgs a) {
     nsel += ts;
     if (tl) {
       uint32_t at = cst.reserve(a, s_hist, tl) + ol;
+      if (lone) {
 #pragma unroll
-      for (int q = 0; q < FILTER_Q; ++q)
-        if ((lone >> q) & 1u) {
-          const uint64_t j = j0 + (uint64_t)q * 32 + lane;
-          cstage[at++] = make_uint2(d[q].x, (uint32_t)(j << a.alpha) + ps[q]);
-        }
+        for (int q = 0; q < FILTER_Q; ++q)
+          if ((lone >> q) & 1u)
+            cstage[at++] = make_uint2(d[q].x, ((j0 + (uint32_t)q * 32u + lane) << a.alpha) + ps[q]);
+      }
     }
     if (ts) {
       if (ns + ts > (uint32_t)SPLIT_STAGE) drain_sel();
       uint32_t at = ns + os;
+      if (sel) {
 #pragma unroll
-      for (int q = 0; q < FILTER_Q; ++q)
-        if ((sel >> q) & 1u) sstage[at++] = (uint32_t)(j0 + (uint64_t)q * 32 + lane);
+        for (int q = 0; q < FILTER_Q; ++q)
+          if ((sel >> q) & 1u) sstage[at++] = j0 + (uint32_t)q * 32u + lane;
+      }
       ns += ts;
     }
   }
@@ -918,69 +927,72 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_gather(FusedArgs a) {
   }
   clear_hist(s_hist, a.nb);
   CandStage cst = {cstage, (uint32_t)GATHER_STAGE, 0u, thr, cand_shift(thr, a.nbits), 0u, 0u, false};
+  // granule and key indices fit 32 bits (n < 2^32); only the round counter
+  // is 64-bit
   const int alpha = a.alpha;
   const int gsh = alpha >= 2 ? 2 : alpha;  // log2 keys per granule
-  const int gk = 1 << gsh;
+  const uint32_t gk = 1u << gsh;
   const int upg = alpha - gsh;             // log2 granules per subrange
-  const uint64_t gmask = (1ull << upg) - 1ull;
+  const uint32_t gmask = (1u << upg) - 1u;
   const uint64_t units = nsub << upg;
-  const uint64_t R = 32ull * GATHER_R;
+  const uint32_t R = 32u * GATHER_R;
   const uint64_t gw = (uint64_t)blockIdx.x * SPLIT_WARPS + wib, nw = (uint64_t)gridDim.x * SPLIT_WARPS;
+  const uint32_t n32 = (uint32_t)a.n;
   // subrange ids of a round's granules; the next round's ids are loaded while
   // this round's keys are in flight
   auto load_ids = [&](uint64_t ub, uint32_t (&sub)[GATHER_R]) {
+    const uint64_t rem = units - ub;  // > 0
+    const uint32_t u32 = (uint32_t)ub;
 #pragma unroll
     for (int r = 0; r < GATHER_R; ++r) {
-      const uint64_t u = ub + (uint64_t)r * 32 + lane;
+      const uint32_t o = (uint32_t)r * 32u + lane;
       sub[r] = 0;
-      if (u < units) sub[r] = ids2 ? __ldg(ids2 + (u >> upg)).y : __ldg(ids1 + (u >> upg));
+      if (o < rem) sub[r] = ids2 ? __ldg(ids2 + ((u32 + o) >> upg)).y : __ldg(ids1 + ((u32 + o) >> upg));
     }
   };
   uint32_t subn[GATHER_R];
   if (gw * R < units) load_ids(gw * R, subn);
   for (uint64_t u0 = gw * R; u0 < units; u0 += nw * R) {
+    const uint64_t rem = units - u0;
+    const uint32_t u32 = (uint32_t)u0;
     uint32_t v[GATHER_R][4];
-    uint32_t kb[GATHER_R];
-    uint32_t sub[GATHER_R];
-#pragma unroll
-    for (int r = 0; r < GATHER_R; ++r) sub[r] = subn[r];
+    uint32_t kb[GATHER_R], lim[GATHER_R];
 #pragma unroll
     for (int r = 0; r < GATHER_R; ++r) {
-      const uint64_t u = u0 + (uint64_t)r * 32 + lane;
-      kb[r] = (uint32_t)(((uint64_t)sub[r] << alpha) + ((u & gmask) << gsh));
+      const uint32_t o = (uint32_t)r * 32u + lane;
+      const uint32_t u = u32 + o;
+      kb[r] = (subn[r] << alpha) + ((u & gmask) << gsh);
+      lim[r] = (o < rem && kb[r] < n32) ? min(gk, n32 - kb[r]) : 0u;  // keys of this granule inside [0, n)
       v[r][0] = v[r][1] = v[r][2] = v[r][3] = 0u;
-      if (u < units) {
-        if (gk == 4 && a.vec_ok && (uint64_t)kb[r] + 4 <= a.n) {
-          const uint4 q = __ldg(reinterpret_cast<const uint4*>(a.keys + kb[r]));
-          v[r][0] = q.x; v[r][1] = q.y; v[r][2] = q.z; v[r][3] = q.w;
-        } else {
+      if (lim[r] == 4u && a.vec_ok) {
+        const uint4 q = __ldg(reinterpret_cast<const uint4*>(a.keys + kb[r]));
+        v[r][0] = q.x; v[r][1] = q.y; v[r][2] = q.z; v[r][3] = q.w;
+      } else {
 #pragma unroll
-          for (int e = 0; e < 4; ++e)
-            if (e < gk && (uint64_t)kb[r] + e < a.n) v[r][e] = __ldg(a.keys + kb[r] + e);
-        }
+        for (int e = 0; e < 4; ++e)
+          if ((uint32_t)e < lim[r]) v[r][e] = __ldg(a.keys + kb[r] + e);
       }
     }
     if (u0 + nw * R < units) load_ids(u0 + nw * R, subn);
     uint32_t take = 0;
 #pragma unroll
-    for (int r = 0; r < GATHER_R; ++r) {
-      const uint64_t u = u0 + (uint64_t)r * 32 + lane;
+    for (int r = 0; r < GATHER_R; ++r)
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         v[r][e] = to_key<KM>(v[r][e]);
-        const bool t = u < units && e < gk && (uint64_t)kb[r] + e < a.n && v[r][e] >= thr;
-        take |= (uint32_t)t << (r * 4 + e);
+        take |= (uint32_t)((uint32_t)e < lim[r] && v[r][e] >= thr) << (r * 4 + e);
       }
-    }
     uint32_t tot = 0;
     const uint32_t off = warp_excl_scan(__popc(take), tot);
     if (tot) {
       uint32_t at = cst.reserve(a, s_hist, tot) + off;
+      if (take) {
 #pragma unroll
-      for (int r = 0; r < GATHER_R; ++r)
+        for (int r = 0; r < GATHER_R; ++r)
 #pragma unroll
-        for (int e = 0; e < 4; ++e)
-          if ((take >> (r * 4 + e)) & 1u) cstage[at++] = make_uint2(v[r][e], kb[r] + e);
+          for (int e = 0; e < 4; ++e)
+            if ((take >> (r * 4 + e)) & 1u) cstage[at++] = make_uint2(v[r][e], kb[r] + e);
+      }
     }
   }
   cst.drain(a, s_hist);
