@@ -168,7 +168,8 @@ def exported_symbols() -> list[str]:
 def params(nbits: int = 8, alpha: int = -1, beta: int = 2, path: int = 0, algo="radix", num_bucket: int = 256,
            largest: bool = True, sorted: bool = False, first_digits: int = 0, team: int = 0) -> Params:
     """team: 0 auto, 1 whole-GPU cooperative grid, 2 one thread-block cluster,
-    3 one CTA with the sets in shared memory, for the phases after the sampler."""
+    3 one CTA with the sets in shared memory, 4 shared GPU (auto, with one cluster
+    of at most 8 CTAs instead of the whole GPU), for the phases after the sampler."""
     p = Params()
     lib().drtopk_params_default(ctypes.byref(p))
     p.nbits, p.alpha, p.beta, p.path, p.team = nbits, alpha, beta, path, team

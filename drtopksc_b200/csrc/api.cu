@@ -523,12 +523,16 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
     if (team == 3) {
       if (!fits || !tail_ready(di->device, P->km)) return DRTOPK_EUNSUPPORTED;
       P->tail = 1;
-    } else if (team == 0 && fits && gather <= TAIL_GATHER_AUTO && cand <= TAIL_CAP / 2 &&
+    } else if ((team == 0 || team == 4) && fits && gather <= TAIL_GATHER_AUTO && cand <= TAIL_CAP / 2 &&
                tail_ready(di->device, P->km)) {
       P->tail = 1;
     } else if (team == 2) {
       P->cluster = cluster_size(di, P->km, smem);
       if (P->cluster <= 0) return DRTOPK_EUNSUPPORTED;
+    } else if (team == 4) {
+      // shared GPU: a portable-size cluster finds room beside other kernels
+      P->cluster = std::min(8, cluster_size(di, P->km, smem));
+      if (P->cluster <= 0) P->cluster = 0;  // no cluster fits: the cooperative grid
     }
     if (P->tail || P->cluster) P->split = P->first_pre = 0;
   }

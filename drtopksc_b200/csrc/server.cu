@@ -6,10 +6,10 @@
 //   * requests with n <= 2^22 and k <= 4096 admitted in the same tick are
 //     grouped into ONE persistent segmented launch (segmented.cuh), each
 //     segment reading and writing its request's own buffers;
-//   * other requests run one select each: in order on one stream when their
-//     tail is the cooperative whole-GPU kernel (one at a time), on a second
-//     stream when it is the one-CTA shared-memory tail, which then overlaps
-//     the other streams' work;
+//   * other requests run one select each, on one of several streams (the
+//     one-CTA shared-memory tail on its own stream), with the phases after
+//     the sampler in one thread-block cluster of at most 8 CTAs rather than
+//     the whole GPU, so that the selects overlap each other's work;
 //   * each request's outputs come back with ONE device-to-host copy on a
 //     third stream, ordered after its kernels by an event, so result copies
 //     never stall the compute streams.
@@ -46,13 +46,19 @@ using namespace drtopk;
 
 namespace {
 
-// stream roles
-constexpr int ST_SINGLE = 0;  // single selects whose tail is a cooperative launch (one at a time)
-constexpr int ST_BATCH = 1;   // micro-batches (segmented kernel, not cooperative)
-constexpr int ST_COPY = 2;    // result copies to pinned host memory and completion events
-constexpr int ST_TAIL = 3;    // single selects with the one-CTA shared-memory tail (not cooperative),
-                              // overlapping the other streams' work on the device
-constexpr int NSTREAMS = 4;
+// stream roles: compute streams, each paired with its own copy stream for
+// the result copies and completion events (a request's copy waits only for
+// its own stream's kernels, never behind another stream's slower request)
+constexpr int ST_BATCH = 0;    // micro-batches (segmented kernel, not cooperative)
+constexpr int ST_TAIL = 1;     // single selects with the one-CTA shared-memory tail
+constexpr int ST_SINGLE = 2;   // first of NSINGLE streams for the other single selects, dealt
+                               // round-robin: their phases after the sampler run in one
+                               // cluster of <= 8 CTAs (team 4), so several overlap each other
+                               // and the other streams' work on the device
+constexpr int NSINGLE = 4;
+constexpr int NCOMPUTE = ST_SINGLE + NSINGLE;
+constexpr int ST_COPY = NCOMPUTE;  // copy stream of compute stream i: ST_COPY + i
+constexpr int NSTREAMS = 2 * NCOMPUTE;
 constexpr uint64_t BATCH_MAX_N = 1ull << 22;  // larger inputs run as single selects
 
 struct Req {
@@ -86,6 +92,8 @@ struct Req {
   double t_submit = 0, t_start = 0, t_done = 0;
   int status = DRTOPK_OK;
   bool small = false;
+  bool planned = false;              // plan computed once, at first admission attempt
+  Plan plan;
 };
 
 // Process-wide cache of pinned host buffers (size classes of powers of two),
@@ -192,23 +200,27 @@ struct drtopk_server {
   int max_inflight = 64;
   drtopk_handle_t h = nullptr;
   cudaStream_t streams[NSTREAMS] = {};
+  uint64_t next_single = 0;  // round-robin over the single-select streams (worker thread only)
   cudaEvent_t ev_kernels = nullptr;  // kernels-done marker (re-recorded per launch)
   int seg_grid = 0;
   size_t seg_smem = 0;
   std::mutex mu;
   std::condition_variable cv, done_cv;
   std::deque<Req*> queue;           // guarded by mu
-  std::list<Req*> running;          // worker thread only
+  std::mutex mu_run;                // guards `launched` and ev_free
+  std::condition_variable cv_run;   // new work for the completion thread
+  std::list<Req*> launched;         // launched, not yet taken by the completion thread
+  std::list<Req*> running;          // completion thread only
   std::deque<drtopk_result_t> results;
   size_t used = 0;
   int inflight = 0;                 // admitted, not yet published (guarded by mu)
   uint64_t next_id = 1;
   bool stop = false;
-  std::thread worker;
+  std::thread worker, completer;
   std::chrono::steady_clock::time_point t0;
   PinnedCache& pinned = pinned_cache();
   DevCache* outs = nullptr;         // this device's process-wide output cache
-  std::vector<cudaEvent_t> ev_free; // worker thread only
+  std::vector<cudaEvent_t> ev_free; // guarded by mu_run
   drtopk_server_stats_t stats = {}; // guarded by mu
   uint64_t pin_allocs0 = 0, pin_ns0 = 0;
 
@@ -216,10 +228,13 @@ struct drtopk_server {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
   cudaEvent_t get_event() {
-    if (!ev_free.empty()) {
-      cudaEvent_t e = ev_free.back();
-      ev_free.pop_back();
-      return e;
+    {
+      std::lock_guard<std::mutex> lk(mu_run);
+      if (!ev_free.empty()) {
+        cudaEvent_t e = ev_free.back();
+        ev_free.pop_back();
+        return e;
+      }
     }
     cudaEvent_t e = nullptr;
     cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
@@ -231,15 +246,20 @@ struct drtopk_server {
     if (!r->dkeys_user) b += al256(r->n * 4);
     b += al256(4) + al256(r->k * 4) + al256(r->k * 8);
     if (!r->small) {
-      drtopk_params_t p;
-      drtopk_params_default(&p);
-      p.alpha = -2;
-      p.sorted = r->sorted;
-      size_t ws = 0;
-      drtopk_status_t s = drtopk_workspace_size(r->n, r->k, r->dtype, &p, &ws);
-      if (s != DRTOPK_OK) return s;
-      r->ws_bytes = ws;
-      b += al256(ws);
+      // the request's one plan: autotuned parameters, shared-GPU team (no
+      // whole-GPU tail, so concurrent selects overlap)
+      if (!r->planned) {
+        drtopk_params_t p;
+        drtopk_params_default(&p);
+        p.alpha = -2;
+        p.sorted = r->sorted;
+        p.team = 4;
+        drtopk_status_t s = plan_select(device, r->n, r->k, r->dtype, &p, r->user_idx != nullptr, &r->plan);
+        if (s != DRTOPK_OK) return s;
+        r->planned = true;
+      }
+      r->ws_bytes = r->plan.ws_bytes;
+      b += al256(r->ws_bytes);
     } else {
       // share of the batch workspace: delegates + candidates of its segment
       b += al256(r->n / 16 * 4) + al256(r->k * 8 * 256);
@@ -252,6 +272,7 @@ struct drtopk_server {
   void finish_on_copy_stream(Req* r, cudaEvent_t kernels_done);
   void admit(std::vector<Req*>& out);
   void launch_admitted(std::vector<Req*>& v);
+  void complete_loop();
   void launch_single(Req* r);
   void launch_batch(std::vector<Req*>& v, int si);
   void loop();
@@ -280,7 +301,10 @@ void drtopk_server::copy_out(Req* r, cudaError_t q) {
   r->hkeys = r->hout = r->extra = nullptr;
   outs->put(r->dout, r->dout_cap);
   r->dout = nullptr;
-  if (r->ev) ev_free.push_back(r->ev);
+  if (r->ev) {
+    std::lock_guard<std::mutex> lk(mu_run);
+    ev_free.push_back(r->ev);
+  }
   r->ev = nullptr;
 }
 
@@ -296,7 +320,7 @@ void drtopk_server::publish(Req* r) {
 // values, indices when asked) on the copy stream after the kernels, then the
 // completion event
 void drtopk_server::finish_on_copy_stream(Req* r, cudaEvent_t kernels_done) {
-  cudaStream_t xs = streams[ST_COPY];
+  cudaStream_t xs = streams[ST_COPY + r->stream];
   cudaStreamWaitEvent(xs, kernels_done, 0);
   if (r->status == DRTOPK_OK && r->dout) {
     const size_t outb = al256(4) + al256(r->k * 4) + (r->user_idx ? al256(r->k * 8) : 0);
@@ -307,16 +331,13 @@ void drtopk_server::finish_on_copy_stream(Req* r, cudaEvent_t kernels_done) {
 
 void drtopk_server::launch_single(Req* r) {
   cudaStream_t st = streams[r->stream];
-  drtopk_params_t p;
-  drtopk_params_default(&p);
-  p.alpha = -2;  // autotuned parameters
-  p.sorted = r->sorted;
   const uint32_t* keys = r->dkeys_user ? static_cast<const uint32_t*>(r->dkeys_user) : r->d_keys;
   if (!r->dkeys_user && cudaMemcpyAsync(r->d_keys, r->hkeys, r->n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
     r->status = DRTOPK_ECUDA;
+  // the plan made at admission, enqueued directly (no per-call statistics)
   if (r->status == DRTOPK_OK)
-    r->status = drtopk_select_ws(h, keys, r->dtype, r->n, r->k, &p, r->d_kth, r->d_vals,
-                                 r->user_idx ? r->d_idx : nullptr, r->d_ws, r->ws_bytes, st);
+    r->status = enqueue_select(r->plan, device, keys, r->d_kth, r->d_vals, r->user_idx ? r->d_idx : nullptr,
+                               r->d_ws, st, nullptr);
   if (r->dmem) cudaFreeAsync(r->dmem, st);  // same stream: reusable by the next request at once
   r->dmem = nullptr;
   cudaEventRecord(ev_kernels, st);
@@ -470,29 +491,20 @@ void drtopk_server::launch_admitted(std::vector<Req*>& v) {
     r->ev = get_event();
     const size_t outb = al256(4) + al256(r->k * 4) + al256(r->k * 8);
     r->hout = pinned.get(outb, &r->hout_cap);
-    r->stream = r->small ? ST_BATCH : ST_SINGLE;
-    if (!r->small) {
-      // a select whose tail is the one-CTA kernel holds few SMs and never
-      // waits on other CTAs: it runs on its own stream, beside the others
-      drtopk_params_t p;
-      drtopk_params_default(&p);
-      p.alpha = -2;
-      p.sorted = r->sorted;
-      Plan P;
-      if (plan_select(device, r->n, r->k, r->dtype, &p, r->user_idx != nullptr, &P) == DRTOPK_OK && P.tail)
-        r->stream = ST_TAIL;
-    }
+    r->stream = r->small ? ST_BATCH : ST_SINGLE + (int)(next_single++ % NSINGLE);
+    // a select whose tail is the one-CTA kernel holds few SMs and never
+    // waits on other CTAs: it runs on its own stream, beside the others
+    if (!r->small && r->plan.tail) r->stream = ST_TAIL;
     cudaStream_t st = streams[r->stream];
     // keys copy (host mode) and, for a request run alone, its workspace
     const size_t kb = r->dkeys_user ? 0 : al256(r->n * 4);
     const size_t dev = kb + (r->small ? 0 : al256(r->ws_bytes));
-    running.push_back(r);
     r->dout = static_cast<char*>(r->hout ? outs->get(outb, &r->dout_cap) : nullptr);
     if (!r->dout || (dev && cudaMallocAsync(reinterpret_cast<void**>(&r->dmem), dev, st) != cudaSuccess)) {
       cudaGetLastError();
       r->dmem = nullptr;
       r->status = DRTOPK_ENOMEM;
-      cudaEventRecord(r->ev, streams[ST_COPY]);
+      cudaEventRecord(r->ev, streams[ST_COPY + r->stream]);
       continue;
     }
     if (!r->dkeys_user) r->d_keys = reinterpret_cast<uint32_t*>(r->dmem);
@@ -507,14 +519,69 @@ void drtopk_server::launch_admitted(std::vector<Req*>& v) {
     else launch_single(r);
   }
   if (!small.empty()) launch_batch(small, ST_BATCH);
+  // hand the requests (all with their completion events recorded) to the
+  // completion thread
+  {
+    std::lock_guard<std::mutex> lk(mu_run);
+    for (Req* r : v) launched.push_back(r);
+  }
+  cv_run.notify_one();
 }
 
+// Launch thread: admission and launches.  Completions run on their own
+// thread (complete_loop), so result copies into the caller's buffers never
+// hold up the next launches.
 void drtopk_server::loop() {
   cudaSetDevice(device);
-  std::vector<Req*> admitted, finished;
+  std::vector<Req*> admitted;
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      if (stop && queue.empty()) break;
+      if (!queue.empty()) admit(admitted);
+      if (inflight == 0) done_cv.notify_all();  // requests refused at admission are already published
+      if (admitted.empty()) {
+        // woken by submit() and by every publish (a slot or budget freed)
+        cv.wait_for(lk, std::chrono::milliseconds(queue.empty() ? 5 : 1));
+        continue;
+      }
+    }
+    const auto tl0 = std::chrono::steady_clock::now();
+    uint64_t ns = 0, nbr = 0;
+    for (Req* r : admitted) (r->small ? nbr : ns)++;
+    launch_admitted(admitted);
+    admitted.clear();
+    const double ms_launch = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl0).count();
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stats.host_ms_launch += ms_launch;
+      stats.singles += ns;
+      stats.batches += nbr ? 1 : 0;
+      stats.batched += nbr;
+      stats.worker_ticks++;
+    }
+  }
+}
+
+// Completion thread: polls the launched requests' completion events, copies
+// finished results into the caller's buffers and publishes them.
+void drtopk_server::complete_loop() {
+  cudaSetDevice(device);
+  std::vector<Req*> finished;
   std::vector<cudaError_t> fq;
   for (;;) {
-    // completions (running is owned by this thread)
+    {
+      std::unique_lock<std::mutex> lk(mu_run);
+      running.splice(running.end(), launched);
+      if (running.empty()) {
+        {
+          std::lock_guard<std::mutex> lk2(mu);
+          if (stop && queue.empty() && inflight == 0) break;
+        }
+        cv_run.wait_for(lk, std::chrono::milliseconds(2));
+        continue;
+      }
+    }
     finished.clear();
     fq.clear();
     for (auto it = running.begin(); it != running.end();) {
@@ -528,39 +595,21 @@ void drtopk_server::loop() {
       fq.push_back(q);
       it = running.erase(it);
     }
+    if (finished.empty()) {
+      std::this_thread::sleep_for(std::chrono::microseconds(10));
+      continue;
+    }
     const auto tc0 = std::chrono::steady_clock::now();
     for (size_t i = 0; i < finished.size(); ++i) copy_out(finished[i], fq[i]);
     const double ms_complete =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc0).count();
     {
-      std::unique_lock<std::mutex> lk(mu);
+      std::lock_guard<std::mutex> lk(mu);
       stats.host_ms_complete += ms_complete;
       for (Req* r : finished) publish(r);
-      if (stop && queue.empty() && inflight == 0) break;
-      if (!queue.empty()) admit(admitted);
-      if (!finished.empty() || inflight == 0) done_cv.notify_all();
-      if (finished.empty() && admitted.empty()) {
-        if (inflight == 0 && queue.empty())
-          cv.wait_for(lk, std::chrono::milliseconds(5));
-        else
-          cv.wait_for(lk, std::chrono::microseconds(20));
-        continue;
-      }
     }
-    const auto tl0 = std::chrono::steady_clock::now();
-    uint64_t ns = 0, nbr = 0;
-    for (Req* r : admitted) (r->small ? nbr : ns)++;
-    if (!admitted.empty()) launch_admitted(admitted);
-    admitted.clear();
-    const double ms_launch = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl0).count();
-    {
-      std::lock_guard<std::mutex> lk(mu);
-      stats.host_ms_launch += ms_launch;
-      stats.singles += ns;
-      stats.batches += nbr ? 1 : 0;
-      stats.batched += nbr;
-      stats.worker_ticks++;
-    }
+    cv.notify_one();
+    done_cv.notify_all();
   }
   done_cv.notify_all();
 }
@@ -604,6 +653,7 @@ extern "C" drtopk_status_t drtopk_server_create(drtopk_server_t* out, int device
   s->pin_allocs0 = s->pinned.allocs.load();
   s->pin_ns0 = s->pinned.alloc_ns.load();
   s->worker = std::thread([s]() { s->loop(); });
+  s->completer = std::thread([s]() { s->complete_loop(); });
   *out = s;
   return DRTOPK_OK;
 }
@@ -622,6 +672,8 @@ extern "C" drtopk_status_t drtopk_server_destroy(drtopk_server_t s) {
   }
   s->cv.notify_all();
   if (s->worker.joinable()) s->worker.join();
+  s->cv_run.notify_all();
+  if (s->completer.joinable()) s->completer.join();
   int cur = 0;
   cudaGetDevice(&cur);
   cudaSetDevice(s->device);

@@ -67,7 +67,9 @@ typedef struct {
   int first_digits; /* beta path: digits used by the first select; 0: reference (32/nbits-3) */
   int team;         /* CTAs running the phases after the sampler: 0 auto, 1 the whole GPU
                        (cooperative grid), 2 one thread-block cluster, 3 one CTA with the sets
-                       in shared memory (small problems) */
+                       in shared memory (small problems), 4 shared GPU: as auto, but a
+                       select that would take the whole GPU runs its phases in one cluster
+                       of at most 8 CTAs, so that concurrent selects overlap (served form) */
 } drtopk_params_t;
 
 typedef struct {
