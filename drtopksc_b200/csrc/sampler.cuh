@@ -236,15 +236,22 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
 #pragma unroll
           for (int e = 0; e < 4; ++e) acc_push<BETA, POS>(acc, k[i][e], (uint32_t)(4 * (gl + G * i) + e));
         for (int off = 1; off < G; off <<= 1) acc_merge<BETA, POS>(acc, acc_shfl_xor<BETA, POS>(acc, off));
-        if (gl == 0) {
+        // the lanes holding a result (gl == 0) own consecutive subranges:
+        // their stores are already coalesced, so they go straight to global
+        // memory (no staging round trip through shared memory)
+        const uint64_t j = ch * (uint64_t)dpc + grp;
+        if (gl == 0 && j < M) {
           if (BETA == 2) {
-            stage[2 * grp] = acc.a1;
-            stage[2 * grp + 1] = acc.a2;
-            if (POS) s_pstage[wib][grp] = (uint16_t)acc.p1;
+            *reinterpret_cast<uint2*>(a.del + 2 * j) = make_uint2(acc.a1, acc.a2);
+            if (POS) a.pos[j] = (uint16_t)acc.p1;
+            emit_hist(acc.a1);
+            emit_hist(acc.a2);
           } else {
-            stage[grp] = acc.a1;
+            a.del[j] = acc.a1;
+            emit_hist(acc.a1);
           }
         }
+        continue;
       } else if (alpha == 3) {
         small_subranges<3, BETA, POS>(k, stage, s_pstage[wib], lane);
       } else if (alpha == 2) {

@@ -367,3 +367,25 @@ def test_split_mode_large_concatenation(dist, n, k, alpha, path):
     _, ost = O.radix_final_kth(x, k, 8, alpha=alpha, path=path)
     assert st["first_threshold"] == ost["first_flag"]
     assert st["n_selected"] == ost["n_selected"]
+
+
+@pytest.mark.parametrize("dist,n,k,alpha,digits,sorted_", [
+    ("u32", 1 << 23, 1 << 15, 3, 2, False), ("u32", 1 << 23, 1 << 15, 3, 2, True),
+    ("f32n", 1 << 23, 1 << 14, 3, 2, False), ("normal", 1 << 23, 1 << 17, 2, 1, False),
+    ("fewdigits", 1 << 22, 1 << 12, 1, 2, False)])
+def test_split_mode_unsorted_and_two_digit_threshold(dist, n, k, alpha, digits, sorted_):
+    """Split mode with the level-1 delegate histogram as its own kernel (two
+    threshold digits), and with unsorted output written by the level-0 split
+    straight into the caller's arrays: same multiset, same lowest-index ties."""
+    x = O.gen(dist, n, 7 * n + k)
+    kth, vals, idx, st = run_topk(x, k, sorted=sorted_, alpha=alpha, path=2, first_digits=digits)
+    ek, ev, ei = expected(x, k, True)
+    if not sorted_:
+        keys = O.as_keys(vals)
+        order = np.lexsort((idx, -keys.astype(np.int64)))
+        vals, idx = vals[order], idx[order]
+    assert same_bits(kth, ek), (dist, k, st)
+    assert same_bits(vals, ev), (dist, k, st)
+    assert np.array_equal(idx, ei), (dist, k, st)
+    assert st["device_error"] == 0
+    assert st["levels_first"] == digits
