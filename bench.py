@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """bench.py -- Dr.Top-k selection throughput on B200.
 
-Workload (the reference's headline config): N = 2^30
+Workload (the reference's headline configuration): N = 2^30
 uint32 keys (4 GiB) drawn uniform over [0, 2^32-1] (seeded Philox on the
 device -- synthetic data standing in for the reference's unseeded
 random_device draws), 8-bit digits, beta = 2, alpha (and path) per k from
@@ -34,7 +34,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 SWEEP = [1 << i for i in range(25)]
-# reference's own published V100S totals (ms) at N=2^30 for some k (optimum_FICO)
+# the reference's own published V100S totals (ms) at N=2^30 for some k (its optimum_FICO results)
 REF_V100S_MS = {1: 7.157, 128: 6.331, 1024: 6.408, 1 << 16: 7.665, 1 << 20: 12.703, 1 << 22: 18.649, 1 << 24: 33.691}
 
 

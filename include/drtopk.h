@@ -39,7 +39,7 @@ typedef enum {
   DRTOPK_ECUDA = 3,        /* CUDA runtime error */
   DRTOPK_EDEVICE = 4,      /* device-side check failed (see drtopk_sync_check) */
   DRTOPK_EBUDGET = 5,      /* request exceeds the handle's / server's HBM budget */
-  DRTOPK_EUNSUPPORTED = 6, /* valid request outside this build's limits */
+  DRTOPK_EUNSUPPORTED = 6, /* valid request outside the library's limits */
   DRTOPK_ETIMEOUT = 7,     /* a bounded device wait gave up */
   DRTOPK_EAGAIN = 8,       /* server: nothing finished yet / queue full */
   DRTOPK_ECANCELLED = 9    /* server: request cancelled */
