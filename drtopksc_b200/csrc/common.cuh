@@ -348,13 +348,6 @@ DRTOPK_DEV Team grid_team(const GridBar& gb) {
   t.cluster = 0;
   return t;
 }
-DRTOPK_DEV Team solo_team() {
-  Team t = {};
-  t.rank = 0;
-  t.size = 1;
-  t.cluster = 2;
-  return t;
-}
 DRTOPK_DEV Team cluster_team() {
   Team t = {};
   t.rank = cluster_ctarank();

@@ -565,19 +565,9 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
 }
 
 // cooperative launch: the whole grid is the team
-constexpr uint32_t SOLO_FINISH_MAX = 32768;  // set sizes one CTA finishes faster than the grid's round trips
-
 template <int KM>
 __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
   extern __shared__ __align__(16) uint32_t s_dyn[];
-  if (a.split0 && !a.sorted && ld_cg_u32(a.C.set_count + 1) <= SOLO_FINISH_MAX) {
-    // after k_split0 the second select goes on with the chosen bin's
-    // members; when they are few, one CTA finishes alone (block barriers
-    // instead of grid barriers).  The count was written by the previous
-    // launch, so every CTA takes the same branch.
-    if (blockIdx.x == 0) fused_body<KM>(a, solo_team(), s_dyn);
-    return;
-  }
   fused_body<KM>(a, grid_team(a.gb), s_dyn);
 }
 
