@@ -148,14 +148,6 @@ DRTOPK_DEV void hist_add_warp(uint32_t* h, uint32_t bin) {
   }
 }
 
-// Histogram increment aggregated over the active lanes that hit the same bin
-// (one atomic per distinct bin): for streams whose bins crowd into a few
-// values without being all equal, such as subrange maxima in the top bins.
-DRTOPK_DEV void hist_add_match(uint32_t* h, uint32_t bin) {
-  const unsigned peers = __match_any_sync(__activemask(), bin);
-  if ((int)lane_id() == __ffs(peers) - 1) atomicAdd(&h[bin], (uint32_t)__popc(peers));
-}
-
 // Block-aggregated append to two lists: every thread of the block passes the
 // number of items it will write to list A and list B (each < 2^16 summed
 // over the block); one atomic per list per call; returns this thread's

@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
   uint32_t mm_lo = 0, mm_hi = 0;  // lane-local max(~v), max(v) of emitted delegates
 
   auto emit_hist = [&](uint32_t v) {
-    if (a.hmode == 1) hist_add_match(s_hist, v >> dshift);
+    if (a.hmode == 1) hist_add_warp(s_hist, v >> dshift);
     else if (a.hmode == 2) { mm_lo = max(mm_lo, ~v); mm_hi = max(mm_hi, v); }
   };
 

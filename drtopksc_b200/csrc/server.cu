@@ -6,10 +6,10 @@
 //   * requests with n <= 2^22 and k <= 4096 admitted in the same tick are
 //     grouped into ONE persistent segmented launch (segmented.cuh), each
 //     segment reading and writing its request's own buffers;
-//   * other requests run one select each, on one of several streams (the
-//     one-CTA shared-memory tail on its own stream), with the phases after
-//     the sampler in one thread-block cluster of at most 8 CTAs rather than
-//     the whole GPU, so that the selects overlap each other's work;
+//   * other requests run one select each: in order on the select stream
+//     (the whole-GPU cooperative tail: one at a time), or on a stream of
+//     their own when their tail is the one-CTA shared-memory kernel, which
+//     then overlaps the other streams' work;
 //   * each request's outputs come back with ONE device-to-host copy on the
 //     copy stream paired with its compute stream, ordered after its kernels
 //     by an event, so result copies never stall the compute streams.
@@ -51,11 +51,18 @@ namespace {
 // its own stream's kernels, never behind another stream's slower request)
 constexpr int ST_BATCH = 0;    // micro-batches (segmented kernel, not cooperative)
 constexpr int ST_TAIL = 1;     // single selects with the one-CTA shared-memory tail
-constexpr int ST_SINGLE = 2;   // first of NSINGLE streams for the other single selects, dealt
-                               // round-robin: their phases after the sampler run in one
-                               // cluster of <= 8 CTAs (team 4), so several overlap each other
-                               // and the other streams' work on the device
-constexpr int NSINGLE = 4;
+constexpr int ST_SINGLE = 2;   // first of NSINGLE streams for the other single selects (dealt
+                               // round-robin when NSINGLE > 1)
+// Single selects run in order on one stream with the planner's own team
+// choice (the whole-GPU cooperative tail for large problems: one at a time).
+// Four streams with the shared-GPU team (SINGLE_TEAM 4: each tail in one
+// 8-CTA cluster, overlapping the other streams' samplers) reached 14-17 K
+// req/s on the bench mix against ~11.5 K, but under saturation a cluster
+// launch could wait seconds for 8 free SMs of one GPC while the other
+// streams' samplers kept arriving (p99 1.7-2.7 s, 0.7-1.2 K req/s in two
+// runs), so it is not the default.
+constexpr int NSINGLE = 1;
+constexpr int SINGLE_TEAM = 0;
 constexpr int NCOMPUTE = ST_SINGLE + NSINGLE;
 constexpr int ST_COPY = NCOMPUTE;  // copy stream of compute stream i: ST_COPY + i
 constexpr int NSTREAMS = 2 * NCOMPUTE;
@@ -247,14 +254,13 @@ struct drtopk_server {
     if (!r->dkeys_user) b += al256(r->n * 4);
     b += al256(4) + al256(r->k * 4) + al256(r->k * 8);
     if (!r->small) {
-      // the request's one plan: autotuned parameters, shared-GPU team (no
-      // whole-GPU tail, so concurrent selects overlap)
+      // the request's one plan: autotuned parameters, SINGLE_TEAM
       if (!r->planned) {
         drtopk_params_t p;
         drtopk_params_default(&p);
         p.alpha = -2;
         p.sorted = r->sorted;
-        p.team = 4;
+        p.team = SINGLE_TEAM;
         drtopk_status_t s = plan_select(device, r->n, r->k, r->dtype, &p, r->user_idx != nullptr, &r->plan);
         if (s != DRTOPK_OK) return s;
         r->planned = true;
