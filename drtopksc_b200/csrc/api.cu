@@ -613,9 +613,11 @@ static cudaError_t launch_sampler_km(const Plan& P, const SampleArgs& sa, int be
   return launch_sample(P.km, sa, beta, P.has_pos, P.sample_grid, st);
 }
 
-static drtopk_status_t launch_coop(void* fn, const Plan& P, void* argp, cudaStream_t st) {
+constexpr int PHASE3_GRID = 64;  // CTAs of the split-mode phase-3 launch (unsorted output)
+
+static drtopk_status_t launch_coop(void* fn, const Plan& P, void* argp, cudaStream_t st, int grid = 0) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(P.fused_grid);
+  cfg.gridDim = dim3(grid > 0 ? grid : P.fused_grid);
   cfg.blockDim = dim3(FUSED_THREADS);
   cfg.dynamicSmemBytes = P.fused_smem;
   cfg.stream = st;
@@ -834,7 +836,12 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
     if (s == DRTOPK_OK) {
       a.phase_lo = 3;
       a.phase_hi = 3;
-      s = launch_coop(fused_ptr(P.km), P, &a, st);
+      // after k_split0 the unsorted second select goes on with one bin's
+      // members and copies the few later entries: round trips, not bytes,
+      // so a smaller team (cheaper grid barriers and histogram flushes)
+      const int g3 = (a.split0 && !P.sorted) ? std::min(P.fused_grid, PHASE3_GRID) : P.fused_grid;
+      a.gb.nblocks = (uint32_t)g3;
+      s = launch_coop(fused_ptr(P.km), P, &a, st, g3);
     }
   }
   if (ev) cudaEventRecord(ev[2], st);
