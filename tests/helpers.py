@@ -63,3 +63,29 @@ def sort_pairs(vals, idx, x_dtype, largest=True):
         keys = ~keys
     order = np.lexsort((idx, -keys.astype(np.int64)))
     return np.asarray(vals)[order], np.asarray(idx)[order]
+
+
+def tie_fill_ambiguous(keys: np.ndarray, alpha: int, k: int) -> bool:
+    """Default path: whether the reference's race-ordered tie fill
+    (FillWithKElementsID, radixselect.cuh:602-618) could keep other subranges
+    than the lowest-id ones kept here.  Its first select stops at a digit
+    whose bin holds one delegate (then one subrange ties) or runs every digit
+    (then the flag is the exact k-th delegate): the fill is ambiguous only
+    when more subranges share that k-th delegate than the fill needs."""
+    d = O.sample_max(keys, alpha)
+    kd = np.partition(d, d.size - k)[d.size - k]
+    return int((d == kd).sum()) > k - int((d > kd).sum())
+
+
+def reference_counters_match(keys, case, got, alpha, k):
+    """Compare (CountSelectedSubrange, CountLonelyElements, write_pos) with a
+    reference fixture; returns the list of mismatches (empty when equal)."""
+    dflt = case["path"] == "D"
+    bad = []
+    if not (got[0] == case["count_selected"] or (dflt and case["count_selected"] > k and got[0] == k)):
+        bad.append(("count_selected", got[0], case["count_selected"]))
+    if got[1] != case["count_lonely"]:
+        bad.append(("count_lonely", got[1], case["count_lonely"]))
+    if got[2] != case["write_pos"] and not (dflt and tie_fill_ambiguous(keys, alpha, k)):
+        bad.append(("write_pos", got[2], case["write_pos"]))
+    return bad

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
+from tests.helpers import reference_counters_match
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "ref_radix_kth.json")
 
@@ -89,5 +90,9 @@ def test_oracle_matches_reference_golden_kth():
         assert kth == c["kth"], c
         assert st["alpha"] == c["alpha"]
         assert ("B" if st["beta_path"] else "D") == c["path"]
+        # the reference's stage counters (radixselect.cuh:585, 1870-1880)
+        if "write_pos" in c:
+            got = (st["n_selected"], st["n_lonely"] if st["beta_path"] else 0, st["n_candidates"])
+            assert not reference_counters_match(O.as_keys(x), c, got, c["alpha"], c["k"]), (c, got)
         checked += 1
     assert checked >= 20
