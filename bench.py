@@ -12,9 +12,12 @@ keys.  metric: keys/s = 25 * N * steps / device time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
---impl reference times the reference path's CPU form (the oracle port: a
-multi-threaded nth_element top-k on the host cores, the reference itself
-having no CPU implementation) on a bounded sample of the same workload.
+--impl reference times the reference's own implementation of the path --
+sample_radix_select from baseline+filter+beta+shuffle/radixselect.cuh, a
+CUDA program, built from its sources for sm_100a by `make -C oracle ref`
+(oracle/_ref/ref_harness) -- on the same workload with its stock parameters,
+and prints the same metric.  Both arms carry the same cpu_baseline: the
+multi-threaded host top-k (oracle port) on one bounded 2^26-key sample.
 Under torchrun (N > 1) every rank runs an independent replica on its own
 GPU (the select does not shard; value = sum over ranks, time = max over
 ranks).
@@ -288,41 +291,112 @@ def bench_served(D, torch, dev, stream, args):
     return out
 
 
+METRIC = "keys/s (exact top-k over N=2^30 uint32 uniform keys, k sweep 2^0..2^24)"
+
+
+def sweep_config(n, nks, world):
+    """The workload both arms measure (identical dicts, so the two lines compare)."""
+    return {"workload": "Dr.Top-k radix top-k, N=2^%d uint32 uniform over [0, 2^32-1], k=2^0..2^24 (one step = "
+                        "the 25-k sweep), nbits=8, beta=2" % (n.bit_length() - 1),
+            "n": n, "ks": nks, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "input 4 GiB >> 126 MB L2 (no flush needed)"}
+
+
+def cpu_baseline(budget_s: float = 15.0):
+    """The multi-threaded host top-k (oracle port: per-thread nth_element +
+    merge + sort) on the box's host cores, on one bounded sample that both
+    arms share: 2^26 seeded uniform uint32 keys, k in {1, 2^10, 2^16, 2^20}."""
+    import numpy as np
+    rng = np.random.default_rng(12345)
+    sample = rng.integers(0, 1 << 32, size=1 << 26, dtype=np.uint64).astype(np.uint32)
+    rate, threads, calls, dt = cpu_topk_rate(sample, [1, 1 << 10, 1 << 16, 1 << 20], budget_s)
+    return {"value": rate, "unit": "keys/s", "cores": threads, "kind": "port",
+            "sample": f"2^26 seeded uniform uint32 keys, k in {{1,2^10,2^16,2^20}}, {calls} calls in {dt:.1f} s "
+                      "(oracle_topk_mt: per-thread nth_element + merge + sort; the reference has no CPU "
+                      "implementation of the path)"}
+
+
 def run_reference(args):
-    """CPU reference arm: rank 0 only."""
+    """Reference arm (rank 0 only): the reference's own sample_radix_select
+    (baseline+filter+beta+shuffle/radixselect.cuh:1782-1894), compiled from
+    its sources for sm_100a into oracle/_ref/ref_harness, timed on this GPU
+    over the same workload with its stock parameters (alpha from main.cu:83,
+    8-bit digits, beta 2) and its stock blocking call.  Without the harness
+    or a GPU, the CPU port stands in for it on a bounded sample."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import numpy as np
-    n_sample = 1 << args.ref_log2n
-    rng = np.random.default_rng(12345)
-    sample = rng.integers(0, 1 << 32, size=n_sample, dtype=np.uint64).astype(np.uint32)
-    ks = [k for k in SWEEP if k <= n_sample]
-    from oracle import oracle as O
-    threads = os.cpu_count() or 1
-    for i in range(args.warmup):
-        O.topk_mt(sample, ks[i % len(ks)], threads)
-    t0 = time.perf_counter()
-    keys = 0
-    for i in range(args.steps):
-        for k in ks:
-            O.topk_mt(sample, k, threads)
-            keys += sample.size
-    dt = time.perf_counter() - t0
-    value = keys / dt
-    out = {
-        "impl": "reference", "metric": "keys/s (exact top-k, k sweep 2^0..2^24)", "value": value, "unit": "keys/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": dt * 1e3 / max(1, args.steps), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded numpy uniform uint32)",
-        "config": {"workload": "uniform uint32 top-k, k sweep 2^0..2^24 (k capped at the sample size)",
-                   "n": n_sample, "sample_of": "N=2^30", "ks": len(ks)},
-        "cpu_baseline": {"value": value, "unit": "keys/s", "cores": threads, "kind": "port",
-                         "sample": f"2^{args.ref_log2n} uniform uint32 keys, {len(ks)} k values per step; "
-                                   "oracle_topk_mt = per-thread nth_element + merge + sort (the reference has no "
-                                   "CPU implementation of the path; its only host check is std::sort)"},
-        "e2e": {"value": value, "unit": "keys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    n = 1 << args.log2n
+    ks = SWEEP if args.ks == "sweep" else [int(x) for x in args.ks.split(",")]
+    ks = [k for k in ks if k <= n]
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    have_gpu = False
+    try:
+        have_gpu = subprocess.run(["nvidia-smi", "-L"], capture_output=True, timeout=60).returncode == 0
+    except (OSError, subprocess.TimeoutExpired):
+        pass
+    out = {"impl": "reference", "metric": METRIC, "unit": "keys/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+           "config": sweep_config(n, len(ks), 1)}
+    if os.access(harness, os.X_OK) and have_gpu:
+        clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+        clocks.start()
+        cmd = [harness, "--bench", "u32", str(args.log2n), ",".join(str(k) for k in ks), "8", "2", "1234",
+               str(args.steps), str(max(3, args.warmup)), str(args.e2e_steps)]
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=3000)
+        ck = clocks.stop()
+        line = [ln for ln in p.stdout.splitlines() if ln.startswith("BENCH ")]
+        if p.returncode != 0 or not line:
+            out["unavailable"] = "reference harness failed: " + (p.stdout + p.stderr)[-300:].replace("\n", " ")
+            print(json.dumps(out), flush=True)
+            return 0
+        r = json.loads(line[0][6:])
+        calls = args.steps * len(ks)
+        ms = r["ms_total"]
+        value = calls * n / (ms * 1e-3)
+        e2e_calls = args.e2e_steps * len(ks)
+        out.update({
+            "value": value, "ms_per_step": ms / args.steps,
+            "data": "synthetic (seeded mt19937 uniform uint32 over [0, 2^32-1], generated on the host)",
+            "params": "alpha per k from the reference formula (main.cu:83), 8-bit digits, beta 2, default path "
+                      "when alpha > 5",
+            "outputs": "the k-th value (the reference returns no top-k list)",
+            "reference": {"kind": "the reference's own GPU code (sample_radix_select) built from its sources for "
+                                  "sm_100a: oracle/_ref/ref_harness --bench",
+                          "per_k": r["per_k"]},
+            "e2e": {"value": e2e_calls * n / (r["e2e_ms_total"] * 1e-3), "unit": "keys/s",
+                    "h2d_bytes_per_step": 4 * n * len(ks), "d2h_bytes_per_step": 4 * len(ks),
+                    "ms_per_step": r["e2e_ms_total"] / max(1, args.e2e_steps),
+                    "note": "per call: H2D of the keys from pinned memory + the reference's blocking call"},
+            "clocks": ck,
+        })
+    else:
+        # no harness or no GPU: the CPU port on a bounded sample of the workload
+        import numpy as np
+        n_sample = 1 << args.ref_log2n
+        rng = np.random.default_rng(12345)
+        sample = rng.integers(0, 1 << 32, size=n_sample, dtype=np.uint64).astype(np.uint32)
+        sks = [k for k in ks if k <= n_sample]
+        from oracle import oracle as O
+        threads = os.cpu_count() or 1
+        for i in range(args.warmup):
+            O.topk_mt(sample, sks[i % len(sks)], threads)
+        t0 = time.perf_counter()
+        keys = 0
+        for _ in range(args.steps):
+            for k in sks:
+                O.topk_mt(sample, k, threads)
+                keys += sample.size
+        dt = time.perf_counter() - t0
+        value = keys / dt
+        out.update({"value": value, "ms_per_step": dt * 1e3 / max(1, args.steps),
+                    "data": "synthetic (seeded numpy uniform uint32)",
+                    "reference": {"kind": f"CPU port on a 2^{args.ref_log2n}-key sample (no reference harness "
+                                          "or no GPU on this host)"},
+                    "e2e": {"value": value, "unit": "keys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    if not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline()
     print(json.dumps(out), flush=True)
     return 0
 
@@ -458,7 +532,8 @@ def main():
                    "frac_of_measured_hbm": (4.0 * n + 4.0 * k) / (kms * 1e-3) / (peak * 1e9),
                    "alpha": st["alpha"], "beta": st["beta"], "candidates": st["n_candidates"],
                    "ms_sample": round(st["ms_sample"], 4), "ms_first": round(st["ms_first"], 4),
-                   "ms_concat": round(st["ms_concat"], 4), "ms_second": round(st["ms_second"], 4)}
+                   "ms_concat": round(st["ms_concat"], 4), "ms_second": round(st["ms_second"], 4),
+                   "launches": st["kernel_launches"]}
             if k in REF_V100S_MS and n == 1 << 30:
                 row["reference_v100s_ms"] = REF_V100S_MS[k]
             out[str(k)] = row
@@ -470,6 +545,8 @@ def main():
         sweep = table(lambda i, k: plist[i])
         if args.alpha_mode == "auto":
             sweep_ref = table(lambda i, k: p_ref)
+    # kernels one step launches (the same plans as the timed sweep)
+    launches_per_step = sum(sweep[str(k)]["launches"] for k in ks) if sweep else None
 
     # ---------------- end to end through the C ABI with host buffers
     e2e = None
@@ -510,13 +587,7 @@ def main():
     # ---------------- CPU baseline (rank 0, N=1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        import numpy as np
-        ns = 1 << 27
-        sample = keys[:ns].cpu().numpy().view(np.uint32).copy()
-        rate, threads, ccalls, cdt = cpu_topk_rate(sample, [1, 1 << 10, 1 << 16, 1 << 20], 15.0)
-        cpu = {"value": rate, "unit": "keys/s", "cores": threads, "kind": "port",
-               "sample": f"first 2^27 keys of the same input, k in {{1,2^10,2^16,2^20}}, {ccalls} calls in "
-                         f"{cdt:.1f} s (oracle_topk_mt: per-thread nth_element + merge + sort)"}
+        cpu = cpu_baseline()
 
     batched = served = None
     if rank == 0 and world == 1:
@@ -531,25 +602,26 @@ def main():
 
     if rank == 0:
         out = {
-            "metric": "keys/s (exact top-k: k-th value + top-k values, k sweep 2^0..2^24, N=2^30)",
+            "metric": METRIC,
             "value": value, "unit": "keys/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u32", "data": "synthetic (seeded torch Philox, uniform uint32 over [0, 2^32-1])",
-            "config": {"workload": "Dr.Top-k radix, N=2^%d uint32 uniform, k=2^0..2^24 (one step = the sweep), "
-                                   "nbits=8, beta=2, alpha per k: %s" % (args.log2n, "autotuner" if args.alpha_mode == "auto"
-                                                                          else "reference formula"),
-                       "n": n, "ks": len(ks), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "input 4 GiB >> 126 MB L2 (no flush needed)"},
+            "config": sweep_config(n, len(ks), world),
+            "params": "alpha, path and threshold digits per k: %s" % (
+                "autotuner (drtopk_autotune)" if args.alpha_mode == "auto" else "reference formula (main.cu:83)"),
+            "outputs": "the k-th value and the k largest values (unsorted), per call",
             "roofline": {"bound": "hbm", "kernel": "k_sample (delegate sampler)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic_bytes, "algorithmic_bytes_per_launch": 4 * n,
                          "ms_per_launch": sample_ms_per_launch,
                          "fused_ms_per_call": ms_fused / max(1, ncalls),
-                         "whole_call_frac": (4.0 * n) / (ms / calls * 1e-3) / (peak * 1e9)},
+                         "whole_call_frac": (4.0 * n) / (ms / calls * 1e-3) / (peak * 1e9),
+                         "per_k_ms": [sweep[str(k)]["ms"] for k in ks] if sweep else None,
+                         "per_k_frac": [round(sweep[str(k)]["frac_of_measured_hbm"], 4) for k in ks] if sweep else None},
             "cpu_baseline": cpu,
             "clocks": ck,
             "e2e": e2e,
-            "gpu_launches": 2 * calls,
+            "gpu_launches": launches_per_step * args.steps if launches_per_step else None,
             "k_sweep": sweep,
             "k_sweep_reference_alpha": sweep_ref,
             "batched": batched,
