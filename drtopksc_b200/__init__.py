@@ -55,7 +55,7 @@ class Stats(ctypes.Structure):
                 ("levels_first", ctypes.c_int), ("levels_second", ctypes.c_int), ("device_error", ctypes.c_uint32),
                 ("ms_sample", ctypes.c_double), ("ms_first", ctypes.c_double), ("ms_concat", ctypes.c_double),
                 ("ms_second", ctypes.c_double), ("ms_total", ctypes.c_double), ("team_ctas", ctypes.c_int),
-                ("team_cluster", ctypes.c_int)]
+                ("team_cluster", ctypes.c_int), ("kernel_launches", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -102,6 +102,9 @@ def lib() -> ctypes.CDLL:
             "drtopk_workspace_size": (st, [u64, u64, i32, P(Params), P(sz)]),
             "drtopk_select": (st, [vp, vp, i32, u64, u64, P(Params), vp, vp, vp, vp]),
             "drtopk_select_ws": (st, [vp, vp, i32, u64, u64, P(Params), vp, vp, vp, vp, sz, vp]),
+            "drtopk_select_noalloc": (st, [vp, i32, u64, u64, P(Params), vp, vp, vp, vp]),
+            "drtopk_noalloc_sync_check": (st, [vp]),
+            "drtopk_load_dataset": (st, [ctypes.c_char_p, i32, u64, P(ctypes.c_uint32), P(ctypes.c_uint64)]),
             "drtopk_sync_check": (st, [vp, vp]),
             "drtopk_last_stats": (st, [vp, P(Stats)]),
             "drtopk_autotune": (st, [u64, u64, i32, P(Params)]),
@@ -303,14 +306,34 @@ def topk(keys, k: int, **kw):
     return default_handle(keys.device.index or 0).topk(keys, k, **kw)
 
 
+# ----------------------------------------------------------------- real-dataset readers
+DATASET_BIN_I32, DATASET_TXT_REF, DATASET_TXT_SCORE = 0, 1, 2
+_FORMATS = {"bin": DATASET_BIN_I32, "txt": DATASET_TXT_REF, "score": DATASET_TXT_SCORE}
+
+
+def load_dataset(path: str, n: int, fmt="txt"):
+    """Keys of a score file as the reference's real-dataset build reads them
+    (RealDatasets/BinaryDataset/main.cu:109-148; drtopk_load_dataset):
+    returns (uint32 numpy array of n keys, values read from the file)."""
+    import numpy as np
+    code = _FORMATS[fmt] if isinstance(fmt, str) else int(fmt)
+    out = np.empty(n, dtype=np.uint32)
+    got = ctypes.c_uint64(0)
+    check(lib().drtopk_load_dataset(os.fsencode(path), code, n, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                    ctypes.byref(got)), "drtopk_load_dataset")
+    return out, got.value
+
+
 # ----------------------------------------------------------------- reference-shaped wrappers
 def sample_radix_select(vec_d, num_element: int, k: int, num_bucket: int, NBitsperDigit: int, CurrentDigit: int,
                         NSubranges: int, SubRangesize: int, alpha: int, Max_d, beta: int = 2,
-                        defaultContribution: bool | None = None, counters=None):
+                        defaultContribution: bool | None = None, counters=None, SubrangeId_d=None):
     """Mirror of sample_radix_select (radixselect.cuh:1782): returns
     (TopKElement, (sample, first, second, concat) seconds).  Max_d receives
-    the delegates; counters, if given, is an int32 CUDA tensor of 3 that
-    receives (CountSelectedSubrange, CountLonelyElements, write_pos)."""
+    the delegates and SubrangeId_d (int32 CUDA tensor, optional) their
+    subrange ids; counters, if given, is an int32 CUDA tensor of 3 that
+    receives the reference's (CountSelectedSubrange, CountLonelyElements,
+    write_pos) -- zero it before the call, as the reference's caller does."""
     if defaultContribution is None:
         defaultContribution = alpha > 5
     kth = ctypes.c_uint32(0)
@@ -322,7 +345,8 @@ def sample_radix_select(vec_d, num_element: int, k: int, num_bucket: int, NBitsp
     st = lib().drtopk_sample_radix_select(
         vec_d.data_ptr(), num_element, k, num_bucket, ctypes.byref(kth), NBitsperDigit, CurrentDigit, NSubranges,
         SubRangesize, alpha, ctypes.byref(t[0]), ctypes.byref(t[1]), ctypes.byref(t[2]), ctypes.byref(t[3]),
-        Max_d.data_ptr() if Max_d is not None else None, None, 256 << 5, 8, 3, 32, (256 << 5) // 8,
+        Max_d.data_ptr() if Max_d is not None else None,
+        SubrangeId_d.data_ptr() if SubrangeId_d is not None else None, 256 << 5, 8, 3, 32, (256 << 5) // 8,
         ((256 << 5) // 8) * SubRangesize, 1, (256 << 5) + (256 << 5 >> 5), 256, beta, int(bool(defaultContribution)),
         min(32, SubRangesize), None, c[1], c[2], None, c[0])
     check(st, "drtopk_sample_radix_select")
@@ -341,8 +365,10 @@ def radix_select(vec_d, num_element: int, k: int, num_bucket: int = 256, NBitspe
 
 
 def sample_bucket_select(vec_d, num_element: int, k: int, num_bucket: int, NSubranges: int, SubRangesize: int,
-                         alpha: int, beta: int = 2, defaultContribution: bool | None = None, counters=None):
-    """Mirror of sample_bucket_select (bucketselect_combined.cuh:1279) with exact integer buckets."""
+                         alpha: int, beta: int = 2, defaultContribution: bool | None = None, counters=None,
+                         SubrangeId_d=None):
+    """Mirror of sample_bucket_select (bucketselect_combined.cuh:1279) with exact integer buckets;
+    counters and SubrangeId_d as for sample_radix_select."""
     if defaultContribution is None:
         defaultContribution = alpha > 5
     kth = ctypes.c_uint32(0)
@@ -353,7 +379,8 @@ def sample_bucket_select(vec_d, num_element: int, k: int, num_bucket: int, NSubr
         c = [base, base + 4, base + 8]
     st = lib().drtopk_sample_bucket_select(
         vec_d.data_ptr(), num_element, k, num_bucket, ctypes.byref(kth), NSubranges, SubRangesize, alpha,
-        ctypes.byref(t[0]), ctypes.byref(t[1]), ctypes.byref(t[2]), ctypes.byref(t[3]), None, None, beta,
+        ctypes.byref(t[0]), ctypes.byref(t[1]), ctypes.byref(t[2]), ctypes.byref(t[3]), None,
+        SubrangeId_d.data_ptr() if SubrangeId_d is not None else None, beta,
         int(bool(defaultContribution)), min(32, SubRangesize), 256, (256 << 5) + 256, 256 << 5, None, c[0], c[1],
         c[2], None)
     check(st, "drtopk_sample_bucket_select")

@@ -207,6 +207,11 @@ static cudaError_t bitonic_max_grid(DevInfo* d, int km, size_t smem, int* grid) 
 // ------------------------------------------------------------ planning
 static inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+drtopk_status_t device_error_status(uint32_t err) {
+  if (!err) return DRTOPK_OK;
+  return (err & DE_BARRIER_TIMEOUT) ? DRTOPK_ETIMEOUT : DRTOPK_EDEVICE;
+}
+
 int ref_alpha(double log2n, double k) {
   // baseline+filter+beta+shuffle/main.cu:83, evaluated as the reference does
   return (int)(0.5 * (log2n - std::log(k) / std::log(2.0) + 3));
@@ -931,10 +936,22 @@ extern "C" drtopk_status_t drtopk_sync_check(drtopk_handle_t h, void* stream) {
   if (s == DRTOPK_OK && h->have_last) {
     uint32_t hdr[CTRL_HDR_WORDS];
     s = read_ctrl(h, hdr);
-    if (s == DRTOPK_OK && hdr[CW_ERR]) s = (hdr[CW_ERR] & DE_BARRIER_TIMEOUT) ? DRTOPK_ETIMEOUT : DRTOPK_EDEVICE;
+    if (s == DRTOPK_OK) s = device_error_status(hdr[CW_ERR]);
   }
   cudaSetDevice(cur);
   return s;
+}
+
+// kernels one select of plan P launches (enqueue_select's launch sequence)
+static int plan_launches(const Plan& P) {
+  const bool sampler = P.path != PATH_PLAIN && !(P.path == PATH_BITONIC && P.normal);
+  int n = sampler ? 1 : 0;
+  if (P.path == PATH_BITONIC || P.tail || P.cluster > 0 || !P.split) return n + 1;
+  n += P.first_pre ? (P.first_levels >= 2 ? 1 : 0) : 1;  // k_level_hist, or the cooperative first select
+  if (P.path == PATH_BETA) n += 1;                       // k_filter
+  n += 1;                                                // k_gather
+  if (!P.bucket) n += 1;                                 // k_split0
+  return n + 1;                                          // the cooperative last levels
 }
 
 extern "C" drtopk_status_t drtopk_last_stats(drtopk_handle_t h, drtopk_stats_t* st) {
@@ -973,6 +990,7 @@ extern "C" drtopk_status_t drtopk_last_stats(drtopk_handle_t h, drtopk_stats_t* 
     st->ms_total = ms_all;
     st->team_ctas = P.tail ? TAIL_CLUSTER : (P.cluster > 0 ? P.cluster : P.fused_grid);
     st->team_cluster = P.tail ? 3 : (P.cluster > 0 ? 1 : 0);
+    st->kernel_launches = plan_launches(P);
   }
   cudaSetDevice(cur);
   return s;
@@ -1175,6 +1193,52 @@ static drtopk_status_t blocking_select(const uint32_t* vec_d, uint64_t n, uint64
   return s;
 }
 
+namespace drtopk {
+// SubrangeId_d as the reference's samplers leave it: SubrangeId_d[j] = j
+// (sampleMax, radixselect.cuh:882-918), or SubrangeId_d[2j] =
+// SubrangeId_d[2j+1] = j beside the (Max, Second) pairs
+// (sampleMax_NoReduction_Beta2, :966-1041)
+__global__ void k_subrange_ids(int* ids, uint64_t n_ids, int per) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_ids; i += (uint64_t)gridDim.x * blockDim.x)
+    ids[i] = (int)(i / (uint64_t)per);
+}
+}  // namespace drtopk
+
+// The reference's observable counters after a delegate select, from our
+// stage statistics:
+//   CountSelectedSubrange: subranges whose keys were concatenated
+//     (FindTopKRanges + FillWithKElementsID, radixselect.cuh:412-427,602-618;
+//     FindTopKRanges_beta, :560-598);
+//   CountLonelyElements: beta path only, beta (= 2) per lonely subrange, since
+//     the reference appends (Max, Second) for each (:585); the default path
+//     leaves the caller-zeroed counter alone, as the reference does;
+//   write_pos: the concatenated size, which on the beta path counts both
+//     values appended per lonely subrange (:1870-1880).
+// This build appends only Max for a lonely subrange (Second < threshold
+// cannot reach the top k), so n_candidates + n_lonely is the reference's size.
+static drtopk_status_t write_reference_counters(const Plan& P, const drtopk_stats_t& st, int* SubrangeId_d,
+                                                int* CountSelectedSubrange_d, int* CountLonelyElements_d,
+                                                int* write_pos_d) {
+  const bool beta = P.path == PATH_BETA;
+  const int sel = (int)st.n_selected;
+  const int lonely = (int)(2 * st.n_lonely);
+  const int wpos = (int)(st.n_candidates + (beta ? st.n_lonely : 0));
+  if (CountSelectedSubrange_d && cudaMemcpy(CountSelectedSubrange_d, &sel, 4, cudaMemcpyHostToDevice) != cudaSuccess)
+    return DRTOPK_ECUDA;
+  if (beta && CountLonelyElements_d &&
+      cudaMemcpy(CountLonelyElements_d, &lonely, 4, cudaMemcpyHostToDevice) != cudaSuccess)
+    return DRTOPK_ECUDA;
+  if (write_pos_d && cudaMemcpy(write_pos_d, &wpos, 4, cudaMemcpyHostToDevice) != cudaSuccess) return DRTOPK_ECUDA;
+  if (SubrangeId_d && (P.path == PATH_BETA || P.path == PATH_DEFAULT)) {
+    const int per = beta ? 2 : 1;
+    const uint64_t n_ids = P.M * (uint64_t)per;
+    const int grid = (int)std::min<uint64_t>(4096, (n_ids + 255) / 256);
+    k_subrange_ids<<<grid, 256>>>(SubrangeId_d, n_ids, per);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return DRTOPK_ECUDA;
+  }
+  return DRTOPK_OK;
+}
+
 extern "C" drtopk_status_t drtopk_sample_radix_select(
     uint32_t* vec_d, int num_element, int k, int num_bucket, uint32_t* TopKElement, int NBitsperDigit,
     int CurrentDigit, int NSubranges, int SubRangesize, int alpha, double* timeforMaxsample,
@@ -1184,7 +1248,7 @@ extern "C" drtopk_status_t drtopk_sample_radix_select(
     int NThreadsPerBlock, int beta, int defaultContribution, int NthreadstoworkInreduction,
     int* SelectedSubrangeId_d, int* CountLonelyElements_d, int* write_pos_d, uint32_t* ConcatenatedRange_d,
     int* CountSelectedSubrange_d) {
-  (void)CurrentDigit; (void)SubrangeId_d; (void)NSharedMemoryElements; (void)SizeOfSubWarp;
+  (void)CurrentDigit; (void)NSharedMemoryElements; (void)SizeOfSubWarp;
   (void)pow_size_Subwarp; (void)NSubWarps_InBlock; (void)NSubRangesPerBlock; (void)NElementsPerBlock_ReadFromGlobal;
   (void)TotalBlocksrequired; (void)SizeOfAllocation; (void)NThreadsPerBlock; (void)NthreadstoworkInreduction;
   (void)SelectedSubrangeId_d; (void)ConcatenatedRange_d;
@@ -1204,17 +1268,17 @@ extern "C" drtopk_status_t drtopk_sample_radix_select(
   if (timeforFirstTopK) *timeforFirstTopK = st.ms_first * 1e-3;
   if (timeforConcatenation) *timeforConcatenation = st.ms_concat * 1e-3;
   if (timeForsecondTopK) *timeForsecondTopK = st.ms_second * 1e-3;
-  // the reference's observable counters
-  int cnt[3] = {(int)st.n_selected, (int)st.n_lonely, (int)st.n_candidates};
-  if (CountSelectedSubrange_d) cudaMemcpy(CountSelectedSubrange_d, &cnt[0], 4, cudaMemcpyHostToDevice);
-  if (CountLonelyElements_d) cudaMemcpy(CountLonelyElements_d, &cnt[1], 4, cudaMemcpyHostToDevice);
-  if (write_pos_d) cudaMemcpy(write_pos_d, &cnt[2], 4, cudaMemcpyHostToDevice);
-  // the delegates in the caller's Max_d (the reference leaves them there)
   drtopk_handle_t h;
-  if (Max_d && default_handle(&h) == DRTOPK_OK && h->have_last && h->last_plan.path != PATH_PLAIN) {
-    const Plan& P = h->last_plan;
+  if (default_handle(&h) != DRTOPK_OK || !h->have_last) return DRTOPK_EINVAL;
+  const Plan& P = h->last_plan;
+  drtopk_status_t rs = write_reference_counters(P, st, SubrangeId_d, CountSelectedSubrange_d, CountLonelyElements_d,
+                                                write_pos_d);
+  if (rs != DRTOPK_OK) return rs;
+  // the delegates in the caller's Max_d (the reference leaves them there)
+  if (Max_d && P.path != PATH_PLAIN) {
     size_t bytes = P.M * (P.path == PATH_BETA ? 8 : 4);
-    cudaMemcpy(Max_d, static_cast<char*>(h->ws) + P.off_del, bytes, cudaMemcpyDeviceToDevice);
+    if (cudaMemcpy(Max_d, static_cast<char*>(h->ws) + P.off_del, bytes, cudaMemcpyDeviceToDevice) != cudaSuccess)
+      return DRTOPK_ECUDA;
   }
   return DRTOPK_OK;
 }
@@ -1238,7 +1302,7 @@ extern "C" drtopk_status_t drtopk_sample_bucket_select(
     int NthreadstoworkInreduction, int NThreadsPerBlock, int SizeOfAllocation, int NSharedMemoryElements,
     int* SelectedSubrangeId_d, int* CountSelectedSubrange_d, int* CountLonelyElements_d, int* write_pos_d,
     uint32_t* ConcatenatedRange_d) {
-  (void)Max_d; (void)SubrangeId_d; (void)NthreadstoworkInreduction; (void)NThreadsPerBlock; (void)SizeOfAllocation;
+  (void)Max_d; (void)NthreadstoworkInreduction; (void)NThreadsPerBlock; (void)SizeOfAllocation;
   (void)NSharedMemoryElements; (void)SelectedSubrangeId_d; (void)ConcatenatedRange_d;
   if (!vec_d || !TopKElement || num_element <= 0 || k <= 0 || k > num_element) return DRTOPK_EINVAL;
   if (SubRangesize != (1 << alpha) || NSubranges != num_element / SubRangesize) return DRTOPK_EINVAL;
@@ -1256,11 +1320,10 @@ extern "C" drtopk_status_t drtopk_sample_bucket_select(
   if (timeforFirstTopK) *timeforFirstTopK = st.ms_first * 1e-3;
   if (timeforConcatenation) *timeforConcatenation = st.ms_concat * 1e-3;
   if (timeForsecondTopK) *timeForsecondTopK = st.ms_second * 1e-3;
-  int cnt[3] = {(int)st.n_selected, (int)st.n_lonely, (int)st.n_candidates};
-  if (CountSelectedSubrange_d) cudaMemcpy(CountSelectedSubrange_d, &cnt[0], 4, cudaMemcpyHostToDevice);
-  if (CountLonelyElements_d) cudaMemcpy(CountLonelyElements_d, &cnt[1], 4, cudaMemcpyHostToDevice);
-  if (write_pos_d) cudaMemcpy(write_pos_d, &cnt[2], 4, cudaMemcpyHostToDevice);
-  return DRTOPK_OK;
+  drtopk_handle_t h;
+  if (default_handle(&h) != DRTOPK_OK || !h->have_last) return DRTOPK_EINVAL;
+  return write_reference_counters(h->last_plan, st, SubrangeId_d, CountSelectedSubrange_d, CountLonelyElements_d,
+                                  write_pos_d);
 }
 
 extern "C" drtopk_status_t drtopk_bitonic_topk(const uint32_t* A_d, int N, int k, int alpha, int NormalBitonic,

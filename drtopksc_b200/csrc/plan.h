@@ -65,6 +65,9 @@ drtopk_status_t plan_select(int device, uint64_t n, uint64_t k, drtopk_dtype_t d
 drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, void* d_kth, void* d_vals,
                                int64_t* d_idx, char* ws, cudaStream_t st, cudaEvent_t* ev);
 int ref_alpha(double log2n, double k);
+// status of a device error word: 0 -> OK, a bounded wait that gave up ->
+// ETIMEOUT, any other device-side check -> EDEVICE
+drtopk_status_t device_error_status(uint32_t err);
 // concatenation length (keys) up to which the automatic choice lets one CTA
 // run the phases after the sampler
 constexpr double TAIL_GATHER_AUTO = 32768.0;

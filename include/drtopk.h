@@ -91,6 +91,7 @@ typedef struct {
   double ms_total;
   int team_ctas;             /* CTAs that ran the phases after the sampler */
   int team_cluster;          /* 0: the cooperative grid; 1: one thread-block cluster; 3: one CTA */
+  int kernel_launches;       /* kernels the last select launched (sampler included) */
 } drtopk_stats_t;
 
 typedef struct drtopk_handle* drtopk_handle_t;
@@ -128,14 +129,24 @@ DRTOPK_API drtopk_status_t drtopk_select_ws(drtopk_handle_t h, const void* d_key
  * forbids allocation inside it).  Same inputs, outputs, parameters and
  * results as drtopk_select, on the current device; the scratch is one
  * 32 MiB (33554432-byte) array built into the library, held by every GPU
- * that loads the library until the process exits.
+ * that uses the library until the process exits.
  * Requests whose workspace (drtopk_workspace_size) is larger return
  * DRTOPK_EUNSUPPORTED.  The first call on a device looks the array's
- * address up; make it before capturing any stream work.  Calls share the
- * array: calls whose GPU work overlaps race and must be serialised. */
+ * address up, and with CUDA's lazy module loading (the default) that first
+ * use is also when the 32 MiB are taken from the device: make the first
+ * call at initialisation, before the caller's allocator reserves the device
+ * memory and before capturing any stream work (CUDA_MODULE_LOADING=EAGER
+ * takes the memory at context creation instead).  Calls share the array:
+ * calls whose GPU work overlaps race and must be serialised. */
 DRTOPK_API drtopk_status_t drtopk_select_noalloc(const void* d_keys, drtopk_dtype_t dtype, uint64_t n, uint64_t k,
                                                  const drtopk_params_t* p, void* d_kth, void* d_vals,
                                                  int64_t* d_idx, void* stream);
+
+/* Companion of drtopk_select_noalloc (no counterpart in the reference):
+ * synchronise the stream and report device-side failures of the last
+ * no-allocation select on the current device (a bounded wait that gave up:
+ * DRTOPK_ETIMEOUT; an internal check: DRTOPK_EDEVICE).  Allocates nothing. */
+DRTOPK_API drtopk_status_t drtopk_noalloc_sync_check(void* stream);
 
 /* Synchronise the stream and report device-side failures of the last call
  * (bounded waits that gave up, internal checks). */
@@ -170,9 +181,15 @@ DRTOPK_API drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_
  * ------------------------------------------------------------------- */
 
 /* baseline+filter+beta+shuffle/radixselect.cuh:1782-1784 sample_radix_select.
- * Max_d (NSubranges*beta keys) receives the delegates; *CountSelectedSubrange_d,
- * *CountLonelyElements_d and *write_pos_d receive the number of selected
- * subranges, lonely elements and candidates (the reference's counters).
+ * Max_d (NSubranges*beta keys) receives the delegates ((Max, Second) pairs on
+ * the beta path) and SubrangeId_d their subrange ids, as the reference's
+ * samplers leave them.  The counters receive the reference's values:
+ * *CountSelectedSubrange_d the subranges whose keys were concatenated;
+ * *CountLonelyElements_d (beta path) beta = 2 per subrange with only its Max
+ * at or above the threshold, left untouched on the default path;
+ * *write_pos_d the concatenated size, two per lonely subrange included.
+ * SelectedSubrangeId_d and ConcatenatedRange_d (the reference's scratch,
+ * filled in an unspecified order there) are not written.
  * Stage times are returned in seconds like the reference's wtime() deltas. */
 DRTOPK_API drtopk_status_t drtopk_sample_radix_select(
     uint32_t* vec_d, int num_element, int k, int num_bucket, uint32_t* TopKElement, int NBitsperDigit,
@@ -189,7 +206,9 @@ DRTOPK_API drtopk_status_t drtopk_radix_select(uint32_t* vec_d, int num_element,
                                     int NBitsperDigit, int CurrentDigit);
 
 /* bucket_select/bucketselect_combined.cuh:1279-1280 sample_bucket_select
- * (k is the k of the k-th largest, as at bucket_select/main.cu:166). */
+ * (k is the k of the k-th largest, as at bucket_select/main.cu:166).  The
+ * counters and SubrangeId_d are written as by drtopk_sample_radix_select;
+ * their values follow this build's exact integer buckets. */
 DRTOPK_API drtopk_status_t drtopk_sample_bucket_select(
     uint32_t* vec_d, int num_element, int k, int num_bucket, uint32_t* TopKElement, int NSubranges,
     int SubRangesize, int alpha, double* timeforMaxsample, double* timeforFirstTopK, double* timeForsecondTopK,
@@ -205,6 +224,30 @@ DRTOPK_API drtopk_status_t drtopk_sample_bucket_select(
  * and N>>alpha >= k (sampleBitonic.cu:198-221). */
 DRTOPK_API drtopk_status_t drtopk_bitonic_topk(const uint32_t* A_d, int N, int k, int alpha, int NormalBitonic,
                                     uint32_t* d_topk, int64_t* d_idx, uint32_t* TopKElement);
+
+/* baseline+filter+beta+shuffle/RealDatasets/BinaryDataset/main.cu:109-148:
+ * the reference's score-file readers (host only, no GPU needed).  Fills
+ * h_keys[0..n) with uint32 keys; *n_read (may be NULL) receives the values
+ * read from the file before any repetition.
+ *   DRTOPK_DATASET_BIN_I32    raw little-endian int32 values, kept as their
+ *                             bit patterns (the readBinary build); a short
+ *                             file repeats its last value, as there
+ *   DRTOPK_DATASET_TXT_REF    decimal scores read as the reference's default
+ *                             build reads them ("%f" into its unsigned key
+ *                             slots, then (1 - u) * 10^9 in unsigned 32-bit
+ *                             arithmetic on the float's bit pattern u); at
+ *                             most 2^26 scores, repeated in order up to n
+ *   DRTOPK_DATASET_TXT_SCORE  the same file with the intended map
+ *                             (1 - s) * 1e9 in float, truncated and clamped
+ *                             to [0, 2^32 - 1]
+ * DRTOPK_EINVAL if the file cannot be read or holds no value. */
+typedef enum {
+  DRTOPK_DATASET_BIN_I32 = 0,
+  DRTOPK_DATASET_TXT_REF = 1,
+  DRTOPK_DATASET_TXT_SCORE = 2
+} drtopk_dataset_format_t;
+DRTOPK_API drtopk_status_t drtopk_load_dataset(const char* path, int format, uint64_t n, uint32_t* h_keys,
+                                               uint64_t* n_read);
 
 /* ---------------------------------------------------------------------
  * Batched form: many independent top-k problems in one persistent launch.

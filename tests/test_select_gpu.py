@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests.helpers import expected, run_topk, same_bits, sort_pairs, to_dev
+from tests.helpers import expected, run_topk, same_bits, sort_pairs, tie_fill_ambiguous, to_dev
 
 pytestmark = pytest.mark.gpu
 
@@ -234,7 +234,10 @@ def test_reference_shaped_wrappers():
         want, ost = O.radix_final_kth(x, k, 8)
         assert kth == want
         c = counters.cpu().numpy()
+        # the reference's counters, as the restated reference path counts them
         assert c[0] == ost["n_selected"]
+        assert c[1] == (0 if dflt else ost["n_lonely"])
+        assert c[2] == ost["n_candidates"] or (dflt and tie_fill_ambiguous(x, alpha, k))
         dl = Max_d.cpu().numpy().view(np.uint32)
         if dflt:
             assert np.array_equal(dl[:nsub], O.sample_max(x, alpha))
