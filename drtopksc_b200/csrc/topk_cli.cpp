@@ -5,6 +5,14 @@
 // The data are uniform uint32 from a seeded mt19937 (the reference uses an
 // unseeded random_device); --seed S, --dist u32|normal|fewdigits|f32u|f32n,
 // --algo radix|bucket|plain, --alpha A, --csv FILE, --check are extras.
+//
+// The real-dataset build (RealDatasets/BinaryDataset/main.cu:56-148) takes
+// "log2N k NBitsPerDigit beta scoreFile output_file": with six positional
+// arguments the keys come from scoreFile and the CSV row goes to
+// output_file.  --format txt (default: the reference's default build, "%f"
+// scores and its unsigned arithmetic), bin (raw int32, the readBinary build)
+// or score ((1 - s) * 1e9 in float) picks the reader (drtopk_load_dataset);
+// --input FILE does the same with the four-argument form.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -55,7 +63,7 @@ int main(int argc, char** argv) {
   std::printf("./exe num_element k NBitsPerDigit beta\n");
   std::vector<std::string> pos;
   uint32_t seed = 1;
-  std::string dist = "u32", algo = "radix", csv = "drtopk_b200.csv";
+  std::string dist = "u32", algo = "radix", csv = "drtopk_b200.csv", input, format = "txt";
   int alpha_opt = -1;
   bool check = false;
   for (int i = 1; i < argc; ++i) {
@@ -66,9 +74,23 @@ int main(int argc, char** argv) {
     else if (a == "--alpha" && i + 1 < argc) alpha_opt = std::atoi(argv[++i]);
     else if (a == "--csv" && i + 1 < argc) csv = argv[++i];
     else if (a == "--check") check = true;
+    else if (a == "--input" && i + 1 < argc) input = argv[++i];
+    else if (a == "--format" && i + 1 < argc) format = argv[++i];
     else pos.push_back(a);
   }
+  if (pos.size() == 6) {  // RealDatasets/BinaryDataset/main.cu:58-59: ... scoreFile output_file
+    input = pos[4];
+    csv = pos[5];
+    pos.resize(4);
+  }
   if (pos.size() != 4) { std::printf("wrong input\n"); return 1; }
+  int fmt = -1;
+  if (!input.empty()) {
+    fmt = format == "bin" ? DRTOPK_DATASET_BIN_I32
+                          : (format == "txt" ? DRTOPK_DATASET_TXT_REF
+                                             : (format == "score" ? DRTOPK_DATASET_TXT_SCORE : -1));
+    if (fmt < 0) { std::printf("wrong input\n"); return 1; }
+  }
   const int log2n = std::atoi(pos[0].c_str());
   const long long k = std::atoll(pos[1].c_str());
   const int nbits = std::atoi(pos[2].c_str());
@@ -77,7 +99,17 @@ int main(int argc, char** argv) {
   const uint64_t n = 1ull << log2n;
   std::printf("num_element: %llu\n", (unsigned long long)n);
   std::vector<uint32_t> h(n);
-  gen(dist, seed, h);
+  if (!input.empty()) {
+    uint64_t got = 0;
+    if (drtopk_load_dataset(input.c_str(), fmt, n, h.data(), &got) != DRTOPK_OK) {
+      std::printf("Error! opening SCORE file\n");
+      return 1;
+    }
+    dist = "u32";  // dataset keys are uint32
+    std::printf("read %llu values from %s\n", (unsigned long long)got, input.c_str());
+  } else {
+    gen(dist, seed, h);
+  }
   drtopk_params_t p;
   drtopk_params_default(&p);
   p.nbits = nbits;
