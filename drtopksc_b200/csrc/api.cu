@@ -34,7 +34,6 @@ struct DevInfo {
   int sms = 0;
   int occ_fused[4] = {0, 0, 0, 0};
   size_t occ_fused_smem[4] = {0, 0, 0, 0};
-  int occ_sample = 0;
 };
 
 static std::mutex g_dev_mu;
@@ -47,10 +46,6 @@ static cudaError_t dev_info(int device, DevInfo** out) {
   if (d.device < 0) {
     cudaError_t e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return e;
-    int occ = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernels(KM_U32).sample2pos, SAMPLE_THREADS, 0);
-    if (e != cudaSuccess) return e;
-    d.occ_sample = std::max(1, occ);
     d.device = device;
   }
   *out = &d;
@@ -58,6 +53,29 @@ static cudaError_t dev_info(int device, DevInfo** out) {
 }
 
 static void* fused_ptr(int km) { return const_cast<void*>(kernels(km).fused); }
+
+// the sampler kernel for (key mode, beta, positions, subrange size)
+static const void* sampler_fn(int km, int beta, bool pos, int alpha) {
+  const KernelSet& ks = kernels(km);
+  if (alpha >= 9) return beta == 2 ? (pos ? ks.sample2posw : ks.sample2w) : ks.sample1w;
+  return beta == 2 ? (pos ? ks.sample2pos : ks.sample2) : ks.sample1;
+}
+
+// resident CTAs per SM of a sampler kernel (cached per device)
+static int sampler_occ(int device, const void* fn) {
+  static std::map<std::pair<int, const void*>, int> cache;
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  int& o = cache[std::make_pair(device, fn)];
+  if (o == 0) {
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, SAMPLE_THREADS, 0) != cudaSuccess) {
+      cudaGetLastError();
+      occ = 1;
+    }
+    o = std::max(1, occ);
+  }
+  return o;
+}
 
 static void* fused_cl_ptr(int km) { return const_cast<void*>(kernels(km).fused_cl); }
 
@@ -138,21 +156,30 @@ static bool tail_ready(int device, int km) {
 }
 
 // the ordinary (non-cooperative) kernels of split mode
-enum SplitKernel : int { SK_GATHER = 0, SK_FILTER = 1, SK_LEVEL_HIST = 2, SK_SPLIT0 = 3 };
+enum SplitKernel : int {
+  SK_GATHER = 0, SK_FILTER = 1, SK_LEVEL_HIST = 2, SK_SPLIT0 = 3, SK_EMIT = 4, SK_PRESAMPLE = 5, SK_PRESAMPLE2 = 6
+};
 static void* split_ptr(int km, int which) {
   const KernelSet& ks = kernels(km);
   switch (which) {
     case SK_FILTER: return const_cast<void*>(ks.filter);
     case SK_LEVEL_HIST: return const_cast<void*>(ks.level_hist);
     case SK_SPLIT0: return const_cast<void*>(ks.split0);
+    case SK_EMIT: return const_cast<void*>(ks.emit);
+    case SK_PRESAMPLE: return const_cast<void*>(ks.presample);
+    case SK_PRESAMPLE2: return const_cast<void*>(ks.presample2);
     default: return const_cast<void*>(ks.gather);
   }
 }
 
 // dynamic shared memory of a split-mode kernel: histogram words + warp stages
 static size_t split_smem(int nb, int which) {
+  if (which == SK_PRESAMPLE || which == SK_PRESAMPLE2) return 0;
   const size_t h = (size_t)std::max(nb, 256) * 4;
-  return which == SK_FILTER ? h + SPLIT_FILTER_SMEM : (which == SK_GATHER ? h + SPLIT_GATHER_SMEM : h);
+  if (which == SK_FILTER) return h + SPLIT_FILTER_SMEM;
+  if (which == SK_GATHER) return h + SPLIT_GATHER_SMEM;
+  if (which == SK_EMIT) return (size_t)SPLIT_WARPS * h + SPLIT_GATHER_SMEM;  // a histogram per warp
+  return h;
 }
 
 static cudaError_t split_grid(DevInfo* d, int km, int which, size_t smem, int* grid) {
@@ -272,6 +299,19 @@ drtopk_status_t make_plan(uint64_t n, uint64_t k, drtopk_dtype_t dtype, const dr
     P->fused_grid = fused_grid;
     return DRTOPK_OK;
   }
+  if (p.path == 4 && p.algo == DRTOPK_ALGO_RADIX) {
+    // sampled-threshold concatenation: no delegate vector (alpha unused)
+    P->path = PATH_EMIT;
+    P->alpha = 0;
+    // sampled keys: one 512-key chunk in PRE_STRIDE; the predicted threshold
+    // must keep k scaled to the sample plus a six-sigma margin above it
+    const uint64_t ns_keys = ((n >> 9) / PRE_STRIDE) * 512;
+    const double ks = ns_keys ? (double)k * (double)ns_keys / (double)n : 0.0;
+    const double t = std::ceil(ks + 6.0 * std::sqrt(ks) + 16.0);
+    P->pre_target = (uint32_t)std::min(t, 4294967295.0);
+    P->fused_grid = fused_grid;
+    return DRTOPK_OK;
+  }
   int alpha = p.alpha;
   const bool auto_alpha = alpha < 0;
   if (auto_alpha) {
@@ -288,6 +328,7 @@ drtopk_status_t make_plan(uint64_t n, uint64_t k, drtopk_dtype_t dtype, const dr
     else if (p.path == 1) path = PATH_DEFAULT;
     else if (p.path == 2) path = PATH_BETA;
     else return DRTOPK_EINVAL;
+
     if (path == PATH_BETA && p.beta != 2) return DRTOPK_EINVAL;  // beta 3/4 paths are broken in the reference
     uint64_t S = 1ull << alpha;
     uint64_t M = (n + S - 1) >> alpha;
@@ -332,6 +373,8 @@ void layout(Plan* P, bool want_idx) {
   P->hist_words = std::max(P->nb, 256);
   P->run_words = 3 * P->hist_words + (MAX_LEVELS + 2) + 1 + 4;
   size_t ctrl_words = CTRL_HDR_WORDS + 4 * (size_t)P->run_words + 8 * 256;
+  P->pre_hist_word = ctrl_words;
+  ctrl_words += 512;  // sampled-threshold path: two 256-bin histograms of the key sample
   P->off_ctrl = take(ctrl_words * 4);
   P->ctrl_bytes = ctrl_words * 4;
   uint64_t ncand_cap = 0;
@@ -499,12 +542,27 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
     // picks are made by every k_filter CTA
     P->first_pre = (P->split && P->path == PATH_BETA && !P->bucket && P->first_levels <= 2) ? 1 : 0;
   }
+  if (P->path == PATH_EMIT) {
+    // the streaming pass appends the candidates; the second select runs as
+    // in split mode
+    P->split = 1;
+    if (split_grid(di, P->km, SK_EMIT, split_smem(P->nb, SK_EMIT), &P->emit_grid) != cudaSuccess ||
+        split_grid(di, P->km, SK_SPLIT0, split_smem(P->nb, SK_SPLIT0), &P->split0_grid) != cudaSuccess ||
+        split_grid(di, P->km, SK_PRESAMPLE, 0, &P->presample_grid) != cudaSuccess)
+      return DRTOPK_ECUDA;
+    // persistent grid over the sampled chunks, PRE_ROUND per warp and round
+    const uint64_t nsw = ((n >> 9) / PRE_STRIDE + PRE_ROUND * SPLIT_WARPS - 1) / (PRE_ROUND * SPLIT_WARPS);
+    P->presample_grid =
+        (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)di->sms * PRE_CTAS_PER_SM, nsw));
+    const uint64_t nct = ((n + 511) / 512 + SPLIT_WARPS - 1) / SPLIT_WARPS;
+    P->emit_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)P->emit_grid, nct));
+  }
   // team of the phases after the sampler: one CTA with the sets in shared
   // memory when they are small (their cost is then round trips, not
   // bandwidth), else the whole GPU; a thread-block cluster on request
   P->cluster = 0;
   P->tail = 0;
-  if (P->path != PATH_BITONIC) {
+  if (P->path != PATH_BITONIC && P->path != PATH_EMIT) {
     const int team = p ? p->team : 0;
     const double dn = (double)n, dk = (double)k, S = (double)P->S;
     // delegates, kept list and candidates must fit TAIL_CAP entries, and the
@@ -542,10 +600,16 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
     if (P->tail || P->cluster) P->split = P->first_pre = 0;
   }
   // sampler grid: persistent, capped by the work items
-  if (P->path != PATH_PLAIN && !(P->path == PATH_BITONIC && P->normal)) {
+  if (P->path != PATH_PLAIN && P->path != PATH_EMIT && !(P->path == PATH_BITONIC && P->normal)) {
     uint64_t items = P->alpha >= 9 ? P->M : ((n + 511) >> 9);
     uint64_t ctas = (items + SAMPLE_WARPS - 1) / SAMPLE_WARPS;
-    P->sample_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(ctas, (uint64_t)di->sms * di->occ_sample));
+    const int beta = P->path == PATH_BETA ? 2 : 1;
+    const bool pos = P->path == PATH_BETA && want_idx;
+    // the warp-per-subrange pass streams best with 4 CTAs per SM (more
+    // resident warps measured ~3 % slower at alpha 12-13)
+    int occ = sampler_occ(di->device, sampler_fn(P->km, beta, pos, P->alpha));
+    if (P->alpha >= 9) occ = std::min(occ, 4);
+    P->sample_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(ctas, (uint64_t)di->sms * occ));
   }
   layout(P, want_idx);
   if (dout) *dout = di;
@@ -588,8 +652,7 @@ extern "C" drtopk_status_t drtopk_workspace_size(uint64_t n, uint64_t k, drtopk_
 namespace drtopk {
 
 static cudaError_t launch_sample(int km, SampleArgs sa, int beta, bool pos, int grid, cudaStream_t st) {
-  const KernelSet& ks = kernels(km);
-  const void* fn = beta == 2 ? (pos ? ks.sample2pos : ks.sample2) : ks.sample1;
+  const void* fn = sampler_fn(km, beta, pos, sa.alpha);
   void* args[] = {&sa};
   return cudaLaunchKernel(fn, dim3(grid), dim3(SAMPLE_THREADS), args, 0, st);
 }
@@ -691,6 +754,7 @@ static drtopk_status_t enqueue_bitonic(const Plan& P, const void* d_keys, void* 
     sa.hmode = 0;
     sa.vec_ok = vec_ok;
     sa.del = const_cast<uint32_t*>(b.del);
+    sa.err = cw + CW_ERR;
     if (launch_sampler_km(P, sa, 1, st) != cudaSuccess) return DRTOPK_ECUDA;
   }
   if (ev) cudaEventRecord(ev[1], st);
@@ -736,6 +800,8 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
   a.gb.nblocks = (uint32_t)P.fused_grid;
   a.thr_word = cw + CW_THR;
   a.tail_flag = cw + CW_TAIL;
+  a.pre_hist = cw + P.pre_hist_word;
+  a.pre_target = P.pre_target;
   a.phase_lo = 1;
   a.phase_hi = 3;
   a.out_kth = static_cast<uint32_t*>(d_kth);
@@ -772,6 +838,35 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
     a.sort_buf[1] = reinterpret_cast<uint64_t*>(ws + P.off_sort1);
     a.sort_cnt = reinterpret_cast<uint32_t*>(ws + P.off_sortcnt);
   }
+  // ---- sampled-threshold path: sample, predict, emit, then the second select
+  if (P.path == PATH_EMIT) {
+    if (ev) cudaEventRecord(ev[1], st);
+    void* args[] = {&a};
+    drtopk_status_t s = DRTOPK_OK;
+    if (cudaLaunchKernel(split_ptr(P.km, SK_PRESAMPLE), dim3(P.presample_grid), dim3(FUSED_THREADS), args, 0, st) !=
+            cudaSuccess ||
+        cudaLaunchKernel(split_ptr(P.km, SK_PRESAMPLE2), dim3(P.presample_grid), dim3(FUSED_THREADS), args, 0, st) !=
+            cudaSuccess ||
+        cudaLaunchKernel(split_ptr(P.km, SK_EMIT), dim3(P.emit_grid), dim3(FUSED_THREADS), args,
+                         split_smem(P.nb, SK_EMIT), st) != cudaSuccess)
+      s = DRTOPK_ECUDA;
+    if (s == DRTOPK_OK) {
+      a.split0 = 1;
+      a.direct0 = P.sorted ? 0 : 1;
+      if (cudaLaunchKernel(split_ptr(P.km, SK_SPLIT0), dim3(P.split0_grid), dim3(FUSED_THREADS), args,
+                           split_smem(P.nb, SK_SPLIT0), st) != cudaSuccess)
+        s = DRTOPK_ECUDA;
+    }
+    if (s == DRTOPK_OK) {
+      a.phase_lo = 3;
+      a.phase_hi = 3;
+      const int g3 = !P.sorted ? std::min(P.fused_grid, PHASE3_GRID) : P.fused_grid;
+      a.gb.nblocks = (uint32_t)g3;
+      s = launch_coop(fused_ptr(P.km), P, &a, st, g3);
+    }
+    if (ev) cudaEventRecord(ev[2], st);
+    return s;
+  }
   // ---- sampler
   if (P.path != PATH_PLAIN) {
     SampleArgs sa;
@@ -785,6 +880,7 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
     sa.pos = const_cast<uint16_t*>(a.pos);
     sa.hist = a.A.H[0];
     sa.minmax = cw + CW_DEL_MINMAX;
+    sa.err = cw + CW_ERR;
     const int beta = P.path == PATH_BETA ? 2 : 1;
     if (launch_sampler_km(P, sa, beta, st) != cudaSuccess) return DRTOPK_ECUDA;
   }
@@ -944,6 +1040,7 @@ extern "C" drtopk_status_t drtopk_sync_check(drtopk_handle_t h, void* stream) {
 
 // kernels one select of plan P launches (enqueue_select's launch sequence)
 static int plan_launches(const Plan& P) {
+  if (P.path == PATH_EMIT) return 5;  // k_presample, k_presample2, k_emit, k_split0, k_fused
   const bool sampler = P.path != PATH_PLAIN && !(P.path == PATH_BITONIC && P.normal);
   int n = sampler ? 1 : 0;
   if (P.path == PATH_BITONIC || P.tail || P.cluster > 0 || !P.split) return n + 1;
@@ -1056,17 +1153,19 @@ extern "C" drtopk_status_t drtopk_profile_end(drtopk_handle_t h, double* ms_samp
 //                                 an extra ~2^-8d of the keys (truncation).
 // Subrange counts per bucket follow Poisson(lambda = q' S).
 // Measured delegate-sampler throughput as a fraction of the HBM copy
-// bandwidth on B200 (n = 2^27, no index output), by log2 subrange size alpha
-// (entries 0..16; alpha < 5 is not run on the one-delegate path).  Small
+// bandwidth on B200 (n = 2^30, no index output), by log2 subrange size alpha
+// (entries 0..16; alpha < 4 is not run on the one-delegate path).  Small
 // subranges cost more instructions per key (lane-owned reductions, and the
-// (Max, Second) pair for beta = 2); float keys pay their order-preserving
-// mapping.  Below ~4096 subranges the warp-per-subrange pass does not fill
-// the GPU, which the occupancy factor models.
+// (Max, Second) pair for beta = 2) and more delegate bytes; float keys pay
+// their order-preserving mapping.  A pass that mostly reads runs above the
+// copy bandwidth (which counts a write per byte read).  Below ~4096
+// subranges the warp-per-subrange pass does not fill the GPU, which the
+// occupancy factor models.
 static double sampler_eff(int alpha, bool beta2, bool f32, double M) {
-  static const double u32_b1[17] = {.6, .6, .6, .6, .7, .82, .94, 1, 1, 1, 1, 1, 1, 1, .97, .97, .97};
-  static const double u32_b2[17] = {.5, .5, .53, .75, .8, .8, .94, .93, .89, .97, 1, 1, 1, 1, .97, .97, .97};
-  static const double f32_b1[17] = {.6, .6, .6, .6, .7, .82, .93, .9, .87, .98, .98, .98, .98, .98, .95, .95, .95};
-  static const double f32_b2[17] = {.45, .45, .49, .64, .76, .77, .79, .77, .73, .83, .97, .97, .97, .97, .92, .92, .92};
+  static const double u32_b1[17] = {.6, .6, .6, .6, .93, .93, 1., 1., 1.05, 1.06, 1.09, 1.1, 1.09, 1.1, 1.07, 1.07, 1.05};
+  static const double u32_b2[17] = {.45, .45, .57, .76, .85, .9, .97, 1., .97, 1.05, 1.12, 1.13, 1.1, 1.1, 1.06, 1.05, 1.07};
+  static const double f32_b1[17] = {.6, .6, .6, .6, .92, .91, 1., 1., 1.05, 1.1, 1.1, 1.1, 1.09, 1.09, 1.06, 1.04, 1.07};
+  static const double f32_b2[17] = {.45, .45, .53, .7, .84, .89, .88, .85, .82, .94, 1.09, 1.12, 1.1, 1.1, 1.03, 1.04, 1.06};
   const int a = std::max(0, std::min(alpha, 16));
   double e = beta2 ? (f32 ? f32_b2[a] : u32_b2[a]) : (f32 ? f32_b1[a] : u32_b1[a]);
   if (alpha >= 9) e *= 0.7 + 0.3 * std::min(1.0, M / 4096.0);
@@ -1146,6 +1245,24 @@ extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_
         if (c < best) { best = c; best_alpha = alpha; best_path = 2; best_digits = d; }
       }
     }
+  }
+  // the sampled-threshold path (path 4): one streaming pass that appends
+  // every key at or above a threshold predicted from a 1/64 key sample;
+  // calibrated on B200: the pass streams at ~1.1 of the copy bandwidth,
+  // ~50 us fixed (two sample passes, five launches, the last levels), and
+  // ~73 bytes' worth per candidate (append, level-0 split, last levels).
+  // Candidates: k plus the six-sigma margin plus one 16-bit prefix bin.
+  bool best_emit = false;
+  if (p->algo == DRTOPK_ALGO_RADIX && n >= (1ull << 20)) {
+    const double ks = dk / 64.0;
+    const double cand = dk + 64.0 * (6.0 * std::sqrt(ks) + 16.0) + dn / 65536.0;
+    const double c = 4.0 * dn / 1.1 + 50.0 * TAIL_BYTES_PER_US + 73.0 * cand;
+    if (c < best) { best = c; best_emit = true; }
+  }
+  if (best_emit) {
+    p->path = 4;
+    p->alpha = 0;
+    return DRTOPK_OK;
   }
   if (best_alpha == 0) {  // nothing fits (k close to n): plain select
     p->algo = p->algo == DRTOPK_ALGO_BUCKET ? p->algo : DRTOPK_ALGO_PLAIN_RADIX;

@@ -15,9 +15,15 @@ struct KernelSet {
   const void* level_hist;  // k_level_hist<KM>
   const void* split0;      // k_split0<KM>
   const void* bitonic;     // k_bitonic<KM>
-  const void* sample1;     // k_sample<KM, 1, false>
-  const void* sample2;     // k_sample<KM, 2, false>
-  const void* sample2pos;  // k_sample<KM, 2, true>
+  const void* presample;   // k_presample<KM>   (sampled-threshold path)
+  const void* presample2;  // k_presample2<KM>
+  const void* emit;        // k_emit<KM>
+  const void* sample1;     // k_sample<KM, 1, false, false>  (alpha <= 8)
+  const void* sample2;     // k_sample<KM, 2, false, false>
+  const void* sample2pos;  // k_sample<KM, 2, true, false>
+  const void* sample1w;    // k_sample<KM, 1, false, true>   (alpha >= 9)
+  const void* sample2w;    // k_sample<KM, 2, false, true>
+  const void* sample2posw; // k_sample<KM, 2, true, true>
 };
 
 const KernelSet& kernels_u32();

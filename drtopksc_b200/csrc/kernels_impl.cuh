@@ -21,9 +21,15 @@ KernelSet make_kernel_set() {
   s.level_hist = (const void*)k_level_hist<KM>;
   s.split0 = (const void*)k_split0<KM>;
   s.bitonic = (const void*)k_bitonic<KM>;
-  s.sample1 = (const void*)k_sample<KM, 1, false>;
-  s.sample2 = (const void*)k_sample<KM, 2, false>;
-  s.sample2pos = (const void*)k_sample<KM, 2, true>;
+  s.presample = (const void*)k_presample<KM>;
+  s.presample2 = (const void*)k_presample2<KM>;
+  s.emit = (const void*)k_emit<KM>;
+  s.sample1 = (const void*)k_sample<KM, 1, false, false>;
+  s.sample2 = (const void*)k_sample<KM, 2, false, false>;
+  s.sample2pos = (const void*)k_sample<KM, 2, true, false>;
+  s.sample1w = (const void*)k_sample<KM, 1, false, true>;
+  s.sample2w = (const void*)k_sample<KM, 2, false, true>;
+  s.sample2posw = (const void*)k_sample<KM, 2, true, true>;
   return s;
 }
 

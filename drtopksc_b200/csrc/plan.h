@@ -41,11 +41,14 @@ struct Plan {
   int cluster;         // > 0: phases after the sampler run in one thread-block cluster of this many CTAs
   int tail;            // 1: phases after the sampler run in one CTA with the sets in shared memory
   int split_grid, filter_grid, hist_grid, split0_grid;
+  int emit_grid, presample_grid;  // sampled-threshold path
+  uint32_t pre_target;            // sampled keys required at or above its predicted threshold
   int first_pre;       // split mode: first select in k_level_hist / k_filter (beta, radix, <= 2 levels)
   size_t fused_smem;
   size_t run_words;
   int hist_words;
   size_t off_ctrl, ctrl_bytes;
+  size_t pre_hist_word;  // word offset of the sampled-threshold histograms in the control block
   size_t off_sel;
   size_t off_del, off_pos, off_Atop, off_Acbuf0, off_Acbuf1;
   size_t off_cand, off_Ccbuf0, off_Ctop;

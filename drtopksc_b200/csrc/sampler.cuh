@@ -32,6 +32,7 @@ struct SampleArgs {
   uint16_t* pos;         // beta=2 with positions: offset of Max inside subrange j
   uint32_t* hist;        // [1<<nbits] (hmode 1)
   uint32_t* minmax;      // [2]: [0] = max(~v) (so min = ~[0]), [1] = max(v) (hmode 2)
+  uint32_t* err;         // device error word
 };
 
 constexpr int SAMPLE_THREADS = 256;
@@ -86,19 +87,26 @@ DRTOPK_DEV void load_row4(const SampleArgs& a, uint64_t base, uint64_t pol, bool
   }
 }
 
-// a lane's 16 consecutive keys as 16/2^SA whole subranges of 2^SA keys
+// A lane's 16 consecutive keys as 16/2^SA whole subranges of 2^SA keys
+// (SA <= 3), with the lane's slot i holding its 128-bit word i ^ r (the
+// rotation that makes the shared-memory transpose conflict-free).  The xor
+// keeps every subrange inside one group of slots, so the groups are reduced
+// in slot order and stored at their true subrange index.
 template <int SA, int BETA, bool POS>
-DRTOPK_DEV void small_subranges(const uint32_t (&k)[4][4], uint32_t* stage, uint16_t* pstage, unsigned lane) {
+DRTOPK_DEV void small_subranges(const uint32_t (&k)[4][4], int r, uint32_t* stage, uint16_t* pstage, unsigned lane) {
   constexpr int S_ = 1 << SA, per = 16 >> SA;
 #pragma unroll
   for (int j = 0; j < per; ++j) {
     Acc acc = {0u, 0u, 0u};
+    int sub = 0;
 #pragma unroll
     for (int t = 0; t < S_; ++t) {
-      const int q = j * S_ + t;
-      acc_push<BETA, POS>(acc, k[q >> 2][q & 3], (uint32_t)t);
+      const int q = j * S_ + t;                     // slot-order key index
+      const int key = 4 * ((q >> 2) ^ r) + (q & 3);  // index among the lane's 16 keys
+      sub = key >> SA;
+      acc_push<BETA, POS>(acc, k[q >> 2][q & 3], (uint32_t)(key & (S_ - 1)));
     }
-    const int d = lane * per + j;
+    const int d = (int)lane * per + sub;
     if (BETA == 2) {
       stage[2 * d] = acc.a1;
       stage[2 * d + 1] = acc.a2;
@@ -109,11 +117,19 @@ DRTOPK_DEV void small_subranges(const uint32_t (&k)[4][4], uint32_t* stage, uint
   }
 }
 
-template <int KM, int BETA, bool POS>
-__global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
-  __shared__ uint32_t s_hist[256];
-  __shared__ uint32_t s_stage[SAMPLE_WARPS][256 * BETA];
-  __shared__ uint16_t s_pstage[SAMPLE_WARPS][POS ? 256 : 1];
+// WIDE: subranges of >= 512 keys (alpha >= 9), one warp per subrange;
+// otherwise 512-key chunks of 512/2^alpha subranges (alpha 1..8).  The two
+// are separate kernels so that each gets its own registers, shared memory
+// and occupancy.  Each warp counts the delegates' top digits in its own
+// shared histogram (delegates crowd into a few top bins, so one histogram
+// per CTA made every warp's atomics meet on the same word); the copies are
+// summed once at the end.
+template <int KM, int BETA, bool POS, bool WIDE>
+__global__ void __launch_bounds__(SAMPLE_THREADS, POS ? 2 : 4) k_sample(SampleArgs a) {
+  __shared__ uint32_t s_hist[SAMPLE_WARPS][256];
+  __shared__ uint32_t s_stage[WIDE ? 1 : SAMPLE_WARPS][WIDE ? 1 : 256 * BETA];
+  __shared__ uint16_t s_pstage[WIDE ? 1 : SAMPLE_WARPS][(POS && !WIDE) ? 256 : 1];
+  __shared__ uint4 s_xpose[WIDE ? 1 : SAMPLE_WARPS][WIDE ? 1 : 128];  // per-warp transpose of one 512-key chunk
   __shared__ uint32_t s_mm[2];
 
   const int tid = threadIdx.x;
@@ -122,7 +138,7 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
   const int nb = 1 << a.nbits;
   const int dshift = 32 - a.nbits;
   if (a.hmode == 1)
-    for (int i = tid; i < nb; i += SAMPLE_THREADS) s_hist[i] = 0;
+    for (int i = tid; i < SAMPLE_WARPS * 256; i += SAMPLE_THREADS) (&s_hist[0][0])[i] = 0;
   if (tid < 2) s_mm[tid] = 0;
   __syncthreads();
 
@@ -135,11 +151,11 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
   uint32_t mm_lo = 0, mm_hi = 0;  // lane-local max(~v), max(v) of emitted delegates
 
   auto emit_hist = [&](uint32_t v) {
-    if (a.hmode == 1) hist_add_warp(s_hist, v >> dshift);
+    if (a.hmode == 1) hist_add_warp(s_hist[wib], v >> dshift);
     else if (a.hmode == 2) { mm_lo = max(mm_lo, ~v); mm_hi = max(mm_hi, v); }
   };
 
-  if (alpha >= 9) {
+  if constexpr (WIDE) {
     // ---- one warp per subrange, 512-key chunks
     for (uint64_t j = gwarp; j < M; j += nwarps) {
       const uint64_t b = j << alpha;
@@ -179,32 +195,39 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
       }
     }
   } else {
-    // ---- 512-key chunks holding 512/S subranges (alpha 1..8).  Lane l owns
-    // 16 keys: with G = max(1, S/16) lanes per subrange, its i-th uint4 is
-    // uint4 (l/G)*4G + (l%G) + G*i of the chunk, so for S >= 16 all 16 keys
-    // belong to one subrange (reduced in-lane, then log2(G) xor steps) and
-    // for S < 16 they are 16/S whole subranges (no shuffles).  Accesses stay
-    // within 128-byte runs of 16*G bytes; the loads allocate in L1 so the
-    // second half of a shared sector hits there.
+    // ---- 512-key chunks holding 512/S subranges (alpha 1..8).  Lane l
+    // reduces keys [16 l, 16 l + 16) of the chunk: with G = max(1, S/16)
+    // lanes per subrange its 16 keys belong to one subrange (reduced in-lane,
+    // then log2(G) xor steps), and for S < 16 they are 16/S whole subranges
+    // (no shuffles).  The keys arrive by fully coalesced 128-bit loads (load
+    // i of lane l is the chunk's word 32 i + l, a 512-byte run per warp
+    // instruction) and are regrouped through a 2 KB per-warp shared-memory
+    // transpose; lane l reads its words back in the order (i ^ r), r = (l/2)
+    // mod 4, which puts the 8 lanes of each quarter-warp on 8 distinct 16-byte
+    // bank groups (no conflicts).  Loading the lane's 16 keys directly needs
+    // 64-byte strides between lanes (16 cache lines per warp load) and
+    // measured ~13 % slower even without any compute.
     const uint64_t nchunks = (a.n + 511) >> 9;
     const int G = alpha >= 4 ? min(32, 1 << (alpha - 4)) : 1;
     const int dpc = 512 >> alpha;  // delegates per chunk
     uint32_t* stage = s_stage[wib];
+    uint4* xbuf = s_xpose[wib];
     const int grp = lane / G, gl = lane % G;
-    auto uidx = [&](int i) { return grp * 4 * G + gl + G * i; };  // uint4 index inside the chunk
+    const int r = (int)((lane >> 1) & 3u);
     // a full chunk is kept as raw words while its loads are in flight and
-    // mapped to keys when it is reduced; a partial (last) chunk is mapped at
-    // load time, with positions >= n as key 0
+    // transposed and mapped when it is reduced; a partial (last) chunk is
+    // loaded in the lane layout and mapped at load time, with positions >= n
+    // as key 0
     auto load_chunk = [&](uint64_t ch, uint32_t (&k)[4][4]) {
       const uint64_t cb = ch << 9;
       const bool full = a.vec_ok && (cb + 512 <= a.n);
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        const uint64_t base = cb + 4 * (uint64_t)uidx(i);
         if (full) {
-          uint4 v = ld_l1_v4(a.keys + base, pol);
+          uint4 v = ld_stream_v4(a.keys + cb + 128 * i + 4 * lane, pol);
           k[i][0] = v.x; k[i][1] = v.y; k[i][2] = v.z; k[i][3] = v.w;
         } else {
+          const uint64_t base = cb + 16 * (uint64_t)lane + 4 * (i ^ r);
 #pragma unroll
           for (int e = 0; e < 4; ++e) k[i][e] = (base + e < a.n) ? to_key<KM>(ld_stream_u32(a.keys + base + e, pol)) : 0u;
         }
@@ -223,18 +246,25 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
         for (int e = 0; e < 4; ++e) k[i][e] = kn[i][e];
       const uint64_t chn = ch + nwarps;
       if (chn < nchunks) load_chunk(chn, kn);
-      if (full) {  // map this chunk's raw words now that the next chunk's loads are issued
+      if (full) {
+        // transpose through shared memory (word 32 i + l -> lane l's words),
+        // then map the raw words to keys
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 4; ++i) xbuf[32 * i + lane] = make_uint4(k[i][0], k[i][1], k[i][2], k[i][3]);
+        __syncwarp();
 #pragma unroll
-          for (int e = 0; e < 4; ++e) k[i][e] = to_key<KM>(k[i][e]);
+        for (int i = 0; i < 4; ++i) {
+          const uint4 v = xbuf[4 * lane + (i ^ r)];
+          k[i][0] = to_key<KM>(v.x); k[i][1] = to_key<KM>(v.y); k[i][2] = to_key<KM>(v.z); k[i][3] = to_key<KM>(v.w);
+        }
+        __syncwarp();
       }
       if (alpha >= 4) {
         Acc acc = {0u, 0u, 0u};
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-          for (int e = 0; e < 4; ++e) acc_push<BETA, POS>(acc, k[i][e], (uint32_t)(4 * (gl + G * i) + e));
+          for (int e = 0; e < 4; ++e) acc_push<BETA, POS>(acc, k[i][e], (uint32_t)(16 * gl + 4 * (i ^ r) + e));
         for (int off = 1; off < G; off <<= 1) acc_merge<BETA, POS>(acc, acc_shfl_xor<BETA, POS>(acc, off));
         // the lanes holding a result (gl == 0) own consecutive subranges:
         // their stores are already coalesced, so they go straight to global
@@ -253,11 +283,11 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
         }
         continue;
       } else if (alpha == 3) {
-        small_subranges<3, BETA, POS>(k, stage, s_pstage[wib], lane);
+        small_subranges<3, BETA, POS>(k, r, stage, s_pstage[wib], lane);
       } else if (alpha == 2) {
-        small_subranges<2, BETA, POS>(k, stage, s_pstage[wib], lane);
+        small_subranges<2, BETA, POS>(k, r, stage, s_pstage[wib], lane);
       } else {
-        small_subranges<1, BETA, POS>(k, stage, s_pstage[wib], lane);
+        small_subranges<1, BETA, POS>(k, r, stage, s_pstage[wib], lane);
       }
       __syncwarp();
       // coalesced copy-out of this chunk's delegates (skip subranges >= M)
@@ -284,8 +314,12 @@ __global__ void __launch_bounds__(SAMPLE_THREADS) k_sample(SampleArgs a) {
   }
   __syncthreads();
   if (a.hmode == 1) {
-    for (int i = tid; i < nb; i += SAMPLE_THREADS)
-      if (s_hist[i]) atomicAdd(&a.hist[i], s_hist[i]);
+    for (int i = tid; i < nb; i += SAMPLE_THREADS) {
+      uint32_t c = 0;
+#pragma unroll
+      for (int w = 0; w < SAMPLE_WARPS; ++w) c += s_hist[w][i];
+      if (c) atomicAdd(&a.hist[i], c);
+    }
   } else if (a.hmode == 2 && tid == 0) {
     atomicMax(&a.minmax[0], s_mm[0]);
     atomicMax(&a.minmax[1], s_mm[1]);
