@@ -413,8 +413,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
-    ap.add_argument("--alpha-mode", choices=["auto", "ref"], default="auto",
-                    help="auto: per-k parameters from the autotuner (headline); ref: the reference's alpha formula")
+    ap.add_argument("--alpha-mode", choices=["auto", "ref", "emit"], default="auto",
+                    help="auto: per-k parameters from the autotuner (headline); ref: the reference's alpha formula; "
+                         "emit: the sampled-threshold path for every k")
     ap.add_argument("--no-table", action="store_true", help="skip the per-k tables after the timed region")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-form measurement")
@@ -457,7 +458,10 @@ def main():
     # 8-bit digits, beta=2; alpha (and path / threshold digits) per k from the
     # autotuner, or the reference formula with --alpha-mode ref
     p_ref = D.params()
-    plist = [D.autotune(n, k, D.U32, D.params(alpha=-2)) if args.alpha_mode == "auto" else p_ref for k in ks]
+    if args.alpha_mode == "emit":
+        plist = [D.params(path=4) for k in ks]
+    else:
+        plist = [D.autotune(n, k, D.U32, D.params(alpha=-2)) if args.alpha_mode == "auto" else p_ref for k in ks]
 
     def one_step():
         for i, k in enumerate(ks):
@@ -608,7 +612,8 @@ def main():
             "dtype": "u32", "data": "synthetic (seeded torch Philox, uniform uint32 over [0, 2^32-1])",
             "config": sweep_config(n, len(ks), world),
             "params": "alpha, path and threshold digits per k: %s" % (
-                "autotuner (drtopk_autotune)" if args.alpha_mode == "auto" else "reference formula (main.cu:83)"),
+                {"auto": "autotuner (drtopk_autotune)", "ref": "reference formula (main.cu:83)",
+                 "emit": "sampled-threshold path (path 4) for every k"}[args.alpha_mode]),
             "outputs": "the k-th value and the k largest values (unsorted), per call",
             "roofline": {"bound": "hbm", "kernel": "k_sample (delegate sampler)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,

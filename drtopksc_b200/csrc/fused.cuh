@@ -29,7 +29,7 @@
 
 namespace drtopk {
 
-enum Path : int { PATH_DEFAULT = 0, PATH_BETA = 1, PATH_PLAIN = 2, PATH_BITONIC = 3 };
+enum Path : int { PATH_DEFAULT = 0, PATH_BETA = 1, PATH_PLAIN = 2, PATH_BITONIC = 3, PATH_EMIT = 4 };
 
 constexpr int SMALL_SORT = 4096;  // top-k sorted in one CTA's shared memory up to this k
 
@@ -71,12 +71,14 @@ struct FusedArgs {
   int first_pre;          // split mode: the first select runs in k_level_hist / k_filter
   int split0;             // split mode: level 0 of the second select runs in k_split0
   int direct0;            // ... writing its top entries straight to the (unsorted) output
+  uint32_t* pre_hist;     // [2][256] sampled-threshold path: top / second byte counts of the key sample
+  uint32_t pre_target;    // sampled keys that must lie at or above the predicted threshold
   GridBar gb;
 };
 
 enum StatSlot : int {
   ST_THR1 = 0, ST_NSEL = 1, ST_NLONELY = 2, ST_NCAND = 3, ST_LVA = 4, ST_LVC = 5,
-  ST_TOPA = 6, ST_TOPC = 7, ST_KTH = 8, ST_OK = 9
+  ST_TOPA = 6, ST_TOPC = 7, ST_KTH = 8, ST_OK = 9, ST_FALLBACK = 10
 };
 
 // --------------------------------------------------------------- gathers
@@ -475,7 +477,20 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
   }
   Src sc = {};
   bool pairs;
-  if (a.path == PATH_PLAIN) {
+  // sampled-threshold path: fewer than k keys at or above the predicted
+  // threshold means the prediction overshot the k-th key; the select then
+  // runs over all keys (plain radix), so the answer stays exact
+  const bool emit_fb = a.path == PATH_EMIT && (ld_cg_u32(a.cand_count) < a.k || ld_cg_u32(a.cand_count) > a.cand_cap);
+  if (emit_fb) {
+    zero_words(tm, a.C.H[0], a.nb);
+    if (!team_sync(tm)) return;
+    Src s = {};
+    s.keys = a.keys; s.count = a.n; s.raw_input = 1;
+    hist_pass<KM>(tm, s, false, false, radix_level0(a.nbits, a.k), a.nb, a.C.H[0], s_hist);
+    if (!team_sync(tm)) return;
+    if (lead) a.stats[ST_FALLBACK] = 1;
+  }
+  if (a.path == PATH_PLAIN || emit_fb) {
     sc.keys = a.keys; sc.count = a.n; sc.raw_input = 1;
     pairs = false;
   } else {
@@ -494,13 +509,13 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
   } else {
     // candidates of the sampled paths are all >= thr1 (their level-0
     // histogram was built against this level by the concatenation)
-    L0c = a.path == PATH_PLAIN ? radix_level0(a.nbits, a.k) : cand_level0(thr1, a.nbits, a.k);
+    L0c = (a.path == PATH_PLAIN || emit_fb) ? radix_level0(a.nbits, a.k) : cand_level0(thr1, a.nbits, a.k);
   }
   EngineCfg cc;
   cc.bucket = a.bucket; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
-  cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0; cc.skip_split0 = a.split0;
+  cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0; cc.skip_split0 = emit_fb ? 0 : a.split0;
   // entries k_split0 already wrote to the output (slots [0, c0) of the list)
-  const uint32_t c0 = a.direct0 ? ld_cg_u32(a.C.top_count) : 0u;
+  const uint32_t c0 = (a.direct0 && !emit_fb) ? ld_cg_u32(a.C.top_count) : 0u;
   RunResult rc = run_select<KM>(cc, sc, pairs, a.C, a.CF, L0c, s_hist, tm, s_fast);
   if (!rc.ok) { if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL); return; }
   const uint32_t K = rc.kth;
@@ -510,7 +525,7 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
     if (a.out_kth) a.out_kth[0] = from_key(K, a.km);
     a.stats[ST_THR1] = thr1;
     if (a.path == PATH_DEFAULT) a.stats[ST_NSEL] = a.k;
-    a.stats[ST_NCAND] = a.path == PATH_PLAIN ? (uint32_t)a.n : ld_cg_u32(a.cand_count);
+    a.stats[ST_NCAND] = (a.path == PATH_PLAIN || emit_fb) ? (uint32_t)a.n : ld_cg_u32(a.cand_count);
     if (a.phase_lo <= 1) a.stats[ST_LVA] = lvA;
     a.stats[ST_LVC] = rc.levels;
     a.stats[ST_TOPA] = a.path == PATH_DEFAULT ? ld_cg_u32(a.A.top_count) : 0u;
@@ -998,6 +1013,207 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_gather(FusedArgs a) {
   cst.drain(a, s_hist);
   if (cst.ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
   flush_cand_stats(a, s_hist, cst.mlo, cst.mhi);
+}
+
+// --------------------------------------------------------------- sampled-threshold path
+// For large k the filter and gather of the delegate paths re-read the
+// delegate vector and the kept subranges after the streaming pass.  This
+// path predicts the threshold before the pass instead and makes the pass
+// itself the concatenation.  The concatenation of the beta path at a
+// threshold t -- whole subranges whose Max and Second reach t, the lone Max
+// of subranges where only Max does -- is exactly the set of keys >= t, so
+// the pass appends every key >= t_pred together with its index:
+//   k_presample   top-byte histogram of a strided sample of the keys (one
+//                 512-key chunk in PRE_STRIDE, at a rotating offset);
+//   k_presample2  the byte picked from it, then the second-byte histogram
+//                 of the sampled keys inside it (the sample is L2-resident);
+//   k_emit        t_pred = the 16-bit prefix boundary at which the sample
+//                 holds pre_target keys (k scaled to the sample plus a
+//                 six-sigma margin, set by the host), then one streaming
+//                 pass appending every key >= t_pred, with the level-0
+//                 histogram of the second select, as the gather does.
+// k_split0 and the last levels of k_fused then run as in split mode.  The
+// count of appended keys proves the prediction: at least k of them means
+// t_pred <= the k-th key, so every key of the top k is a candidate.  With
+// fewer, k_split0 does nothing and k_fused selects over all keys (plain
+// radix select), so the result is exact whatever the input.
+constexpr int PRE_STRIDE = 64;
+constexpr int PRE_ROUND = 4;     // sampled chunks in flight per warp
+constexpr int PRE_CTAS_PER_SM = 2;
+
+DRTOPK_DEV uint64_t pre_chunk(uint64_t i) { return i * PRE_STRIDE + ((i * 37u) & (PRE_STRIDE - 1)); }
+
+// 16 keys of 512-key chunk `ch` held by this lane (load q: keys
+// ch*512 + 128 q + 4 lane + e), mapped to keys; positions >= n read as key 0
+template <int KM>
+DRTOPK_DEV void chunk_keys(const FusedArgs& a, uint64_t ch, uint64_t pol, uint32_t (&k)[4][4]) {
+  const uint64_t cb = ch << 9;
+  const unsigned lane = lane_id();
+  const bool full = a.vec_ok && cb + 512 <= a.n;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const uint64_t base = cb + 128 * q + 4 * lane;
+    if (full) {
+      const uint4 v = ld_stream_v4(a.keys + base, pol);
+      k[q][0] = v.x; k[q][1] = v.y; k[q][2] = v.z; k[q][3] = v.w;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) k[q][e] = base + e < a.n ? __ldg(a.keys + base + e) : 0u;
+    }
+  }
+}
+
+template <int KM>
+DRTOPK_DEV void presample_pass(const FusedArgs& a, int level, uint32_t b0, uint32_t (*s_h)[256]) {
+  const unsigned lane = lane_id();
+  const int wib = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < SPLIT_WARPS * 256; i += blockDim.x) (&s_h[0][0])[i] = 0;
+  __syncthreads();
+  const uint64_t ns = (a.n >> 9) / PRE_STRIDE;
+  const uint64_t gw = (uint64_t)blockIdx.x * SPLIT_WARPS + wib, nw = (uint64_t)gridDim.x * SPLIT_WARPS;
+  // PRE_ROUND sampled chunks per warp and round, all loaded before any is
+  // counted (the pass is latency-bound); a small persistent grid keeps the
+  // histogram flushes few
+  for (uint64_t i = gw; i < ns; i += PRE_ROUND * nw) {
+    uint32_t k[PRE_ROUND][4][4];
+#pragma unroll
+    for (int c = 0; c < PRE_ROUND; ++c) {
+      const uint64_t ic = i + (uint64_t)c * nw;
+      const uint64_t cb = pre_chunk(ic < ns ? ic : i) << 9;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint64_t base = cb + 128 * q + 4 * lane;
+        if (a.vec_ok) {
+          const uint4 v = __ldg(reinterpret_cast<const uint4*>(a.keys + base));
+          k[c][q][0] = v.x; k[c][q][1] = v.y; k[c][q][2] = v.z; k[c][q][3] = v.w;
+        } else {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) k[c][q][e] = __ldg(a.keys + base + e);
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < PRE_ROUND; ++c) {
+      if (i + (uint64_t)c * nw >= ns) break;  // warp-uniform
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const uint32_t key = to_key<KM>(k[c][q][e]);
+          if (level == 0) hist_add_warp(s_h[wib], key >> 24);
+          else if ((key >> 24) == b0) atomicAdd(&s_h[wib][(key >> 16) & 255u], 1u);
+        }
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < 256; b += blockDim.x) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int w = 0; w < SPLIT_WARPS; ++w) c += s_h[w][b];
+    if (c) atomicAdd(&a.pre_hist[256 * level + b], c);
+  }
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_presample(FusedArgs a) {
+  __shared__ uint32_t s_h[SPLIT_WARPS][256];
+  if (blockIdx.x == 0 && threadIdx.x == 0) stamp(a.stats, 16);
+  presample_pass<KM>(a, 0, 0u, s_h);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_presample2(FusedArgs a) {
+  __shared__ uint32_t s_h[SPLIT_WARPS][256];
+  const Pick p0 = block_pick<false>(a.pre_hist, 256, a.pre_target);
+  presample_pass<KM>(a, 1, (uint32_t)p0.b, s_h);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_emit(FusedArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  // one histogram copy per warp (candidates crowd into a few bins), summed
+  // before the flush
+  const int hw = split_hist_words(a.nb);
+  const unsigned lane = lane_id();
+  const int wib = threadIdx.x >> 5;
+  uint32_t* s_hist = s_dyn + (size_t)wib * hw;
+  uint2* cstage = reinterpret_cast<uint2*>(s_dyn + (size_t)SPLIT_WARPS * hw) + (size_t)wib * GATHER_STAGE;
+  // the predicted threshold: 16-bit prefix boundary holding pre_target
+  // sampled keys at or above it
+  const Pick p0 = block_pick<false>(a.pre_hist, 256, a.pre_target);
+  const uint32_t r1 = a.pre_target > p0.above ? a.pre_target - p0.above : 1u;
+  const Pick p1 = block_pick<false>(a.pre_hist + 256, 256, r1);
+  const uint32_t thr = ((uint32_t)p0.b << 24) | ((uint32_t)p1.b << 16);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *a.thr_word = thr;
+    a.stats[ST_LVA] = 2;
+    stamp(a.stats, 18);
+  }
+  for (int i = threadIdx.x; i < SPLIT_WARPS * hw; i += blockDim.x) s_dyn[i] = 0;
+  __syncthreads();
+  CandStage cst = {cstage, (uint32_t)GATHER_STAGE, 0u, thr, cand_shift(thr, a.nbits), 0u, 0u, false};
+  const uint64_t pol = make_evict_first_policy();
+  const uint64_t nchunks = (a.n + 511) >> 9;
+  const uint64_t gw = (uint64_t)blockIdx.x * SPLIT_WARPS + wib, nw = (uint64_t)gridDim.x * SPLIT_WARPS;
+  // register double buffer: the next chunk's loads are in flight while this
+  // chunk is compared and compacted
+  uint32_t kn[4][4];
+  uint64_t ch = gw;
+  if (ch < nchunks) chunk_keys<KM>(a, ch, pol, kn);
+  for (; ch < nchunks; ch += nw) {
+    uint32_t k[4][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) k[q][e] = kn[q][e];
+    if (ch + nw < nchunks) chunk_keys<KM>(a, ch + nw, pol, kn);
+    const uint64_t cb = ch << 9;
+    uint32_t take = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        k[q][e] = to_key<KM>(k[q][e]);
+        take |= (uint32_t)(k[q][e] >= thr) << (4 * q + e);
+      }
+    if (cb + 512 > a.n) {  // the partial last chunk: drop positions >= n
+      const uint32_t lim = (uint32_t)(a.n - cb);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (128u * q + 4u * lane + e >= lim) take &= ~(1u << (4 * q + e));
+    }
+    if (!__any_sync(0xffffffffu, take != 0u)) continue;
+    uint32_t tot = 0;
+    const uint32_t off = warp_excl_scan(__popc(take), tot);
+    uint32_t at = cst.reserve(a, s_hist, tot) + off;
+    // few lanes take a key, and rarely more than one: walk the set bits and
+    // pick each key out of the 16 registers with a select tree (no
+    // dynamically indexed register array)
+    const uint32_t i0 = (uint32_t)cb + 4 * lane;
+    for (uint32_t t = take; t; t &= t - 1) {
+      const int b = __ffs(t) - 1;
+      uint32_t s8[8], s4[4], s2[2];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) s8[j] = (b & 1) ? k[(2 * j + 1) >> 2][(2 * j + 1) & 3] : k[(2 * j) >> 2][(2 * j) & 3];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) s4[j] = (b & 2) ? s8[2 * j + 1] : s8[2 * j];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) s2[j] = (b & 4) ? s4[2 * j + 1] : s4[2 * j];
+      const uint32_t key = (b & 8) ? s2[1] : s2[0];
+      cstage[at++] = make_uint2(key, i0 + 128u * (uint32_t)(b >> 2) + (uint32_t)(b & 3));
+    }
+  }
+  cst.drain(a, s_hist);
+  if (cst.ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
+  __syncthreads();
+  for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int w = 0; w < SPLIT_WARPS; ++w) c += s_dyn[(size_t)w * hw + b];
+    if (c) atomicAdd(&a.C.H[0][b], c);
+  }
 }
 
 }  // namespace drtopk

@@ -59,7 +59,10 @@ typedef struct {
   int nbits;        /* bits per radix digit: 1,2,4,8 (reference NBitsPerDigit; default 8) */
   int alpha;        /* log2 subrange size; -1: reference formula (main.cu:83); -2: autotuner */
   int beta;         /* delegates per subrange on the small-alpha path; only 2 is valid (default 2) */
-  int path;         /* 0: reference rule (alpha>5 -> one delegate, else beta delegates); 1: one; 2: beta */
+  int path;         /* 0: reference rule (alpha>5 -> one delegate, else beta delegates); 1: one; 2: beta;
+                       4: sampled threshold (radix only): the streaming pass appends every key at or
+                       above a threshold predicted from a key sample (no delegate vector; exact, with
+                       a plain radix select over all keys when the prediction overshoots) */
   int algo;         /* drtopk_algo_t (default RADIX) */
   int num_bucket;   /* bucket variant: buckets per level, 2..4096 (default 256) */
   int largest;      /* 1: k largest (reference semantics, default); 0: k smallest */
