@@ -65,7 +65,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("singles", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("batched", ctypes.c_uint64),
                 ("pinned_allocs", ctypes.c_uint64), ("worker_ticks", ctypes.c_uint64),
                 ("host_ms_pinned", ctypes.c_double), ("host_ms_launch", ctypes.c_double),
-                ("host_ms_complete", ctypes.c_double)]
+                ("host_ms_complete", ctypes.c_double), ("retries", ctypes.c_uint64), ("host_ms_retry", ctypes.c_double),
+                ("host_ms_alloc", ctypes.c_double)]
 
 
 class Result(ctypes.Structure):

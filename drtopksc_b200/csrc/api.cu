@@ -79,6 +79,38 @@ static int sampler_occ(int device, const void* fn) {
 
 static void* fused_cl_ptr(int km) { return const_cast<void*>(kernels(km).fused_cl); }
 
+static void* fused_one_ptr(int km) { return const_cast<void*>(kernels(km).fused_one); }
+
+// dynamic shared memory limit of the grouped one-CTA last levels
+static bool fused_one_group_ready(int device, int km, size_t smem) {
+  static size_t set[64][4];
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  if (device < 0 || device >= 64) return false;
+  if (set[device][km] >= smem) return true;
+  if (cudaFuncSetAttribute(kernels(km).fused_one_g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  set[device][km] = smem;
+  return true;
+}
+
+// dynamic shared memory limit of the one-CTA last-levels kernel (set once
+// per device and key mode; the largest plan's need)
+static bool fused_one_ready(int device, int km, size_t smem) {
+  static size_t set[64][4];
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  if (device < 0 || device >= 64) return false;
+  if (set[device][km] >= smem) return true;
+  if (cudaFuncSetAttribute(fused_one_ptr(km), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  set[device][km] = smem;
+  return true;
+}
+
 // Largest cluster (16, else 8, else 4) of k_fused_cl CTAs that the device
 // can co-schedule with the largest dynamic shared memory a plan uses
 // (FUSED_CL_SMEM_MAX, set once as the kernel's limit); 0 if none.
@@ -157,7 +189,8 @@ static bool tail_ready(int device, int km) {
 
 // the ordinary (non-cooperative) kernels of split mode
 enum SplitKernel : int {
-  SK_GATHER = 0, SK_FILTER = 1, SK_LEVEL_HIST = 2, SK_SPLIT0 = 3, SK_EMIT = 4, SK_PRESAMPLE = 5, SK_PRESAMPLE2 = 6
+  SK_GATHER = 0, SK_FILTER = 1, SK_LEVEL_HIST = 2, SK_SPLIT0 = 3, SK_EMIT = 4, SK_PRESAMPLE = 5, SK_PRESAMPLE2 = 6,
+  SK_CAND_HIST = 7
 };
 static void* split_ptr(int km, int which) {
   const KernelSet& ks = kernels(km);
@@ -168,6 +201,7 @@ static void* split_ptr(int km, int which) {
     case SK_EMIT: return const_cast<void*>(ks.emit);
     case SK_PRESAMPLE: return const_cast<void*>(ks.presample);
     case SK_PRESAMPLE2: return const_cast<void*>(ks.presample2);
+    case SK_CAND_HIST: return const_cast<void*>(ks.cand_hist);
     default: return const_cast<void*>(ks.gather);
   }
 }
@@ -178,7 +212,7 @@ static size_t split_smem(int nb, int which) {
   const size_t h = (size_t)std::max(nb, 256) * 4;
   if (which == SK_FILTER) return h + SPLIT_FILTER_SMEM;
   if (which == SK_GATHER) return h + SPLIT_GATHER_SMEM;
-  if (which == SK_EMIT) return (size_t)SPLIT_WARPS * h + SPLIT_GATHER_SMEM;  // a histogram per warp
+  if (which == SK_EMIT) return SPLIT_GATHER_SMEM;
   return h;
 }
 
@@ -403,7 +437,7 @@ void layout(Plan* P, bool want_idx) {
     P->off_sel = take(P->M * 4);
     ncand_cap = P->n;
   } else {
-    ncand_cap = P->n;
+    ncand_cap = (P->bounded && P->cap_bound) ? std::min<uint64_t>(P->n, P->cap_bound) : P->n;
   }
   P->cand_cap = ncand_cap;
   P->off_cand = take(ncand_cap * 8);
@@ -548,7 +582,8 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
     P->split = 1;
     if (split_grid(di, P->km, SK_EMIT, split_smem(P->nb, SK_EMIT), &P->emit_grid) != cudaSuccess ||
         split_grid(di, P->km, SK_SPLIT0, split_smem(P->nb, SK_SPLIT0), &P->split0_grid) != cudaSuccess ||
-        split_grid(di, P->km, SK_PRESAMPLE, 0, &P->presample_grid) != cudaSuccess)
+        split_grid(di, P->km, SK_PRESAMPLE, 0, &P->presample_grid) != cudaSuccess ||
+        split_grid(di, P->km, SK_CAND_HIST, split_smem(P->nb, SK_CAND_HIST), &P->hist_grid) != cudaSuccess)
       return DRTOPK_ECUDA;
     // persistent grid over the sampled chunks, PRE_ROUND per warp and round
     const uint64_t nsw = ((n >> 9) / PRE_STRIDE + PRE_ROUND * SPLIT_WARPS - 1) / (PRE_ROUND * SPLIT_WARPS);
@@ -556,6 +591,8 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
         (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)di->sms * PRE_CTAS_PER_SM, nsw));
     const uint64_t nct = ((n + 511) / 512 + SPLIT_WARPS - 1) / SPLIT_WARPS;
     P->emit_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)P->emit_grid, nct));
+    // team 5: every launch an ordinary one, the last levels in one CTA
+    P->one_cta = (p && p->team == 5 && fused_one_ready(di->device, P->km, smem)) ? 1 : 0;
   }
   // team of the phases after the sampler: one CTA with the sets in shared
   // memory when they are small (their cost is then round trips, not
@@ -620,6 +657,20 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
 drtopk_status_t drtopk::plan_select(int device, uint64_t n, uint64_t k, drtopk_dtype_t dtype,
                                     const drtopk_params_t* p, bool want_idx, Plan* P) {
   return plan_for(device, n, k, dtype, p, want_idx, P, nullptr);
+}
+
+drtopk_status_t drtopk::plan_select_bounded(int device, uint64_t n, uint64_t k, drtopk_dtype_t dtype,
+                                            const drtopk_params_t* p, bool want_idx, Plan* P) {
+  drtopk_status_t s = plan_for(device, n, k, dtype, p, want_idx, P, nullptr);
+  if (s != DRTOPK_OK || P->path != PATH_EMIT || !P->one_cta) return s;
+  // twice the expected candidates (k, the six-sigma margin, one 16-bit
+  // prefix bin) plus 64K
+  const double ks = (double)k / 64.0;
+  const double est = (double)k + 64.0 * (6.0 * std::sqrt(ks) + 16.0) + (double)n / 65536.0;
+  P->bounded = 1;
+  P->cap_bound = (uint64_t)(2.0 * est) + 65536;
+  layout(P, want_idx);
+  return DRTOPK_OK;
 }
 
 extern "C" drtopk_status_t drtopk_workspace_size(uint64_t n, uint64_t k, drtopk_dtype_t dtype,
@@ -763,15 +814,13 @@ static drtopk_status_t enqueue_bitonic(const Plan& P, const void* d_keys, void* 
   return s;
 }
 
-drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, void* d_kth, void* d_vals,
-                               int64_t* d_idx, char* ws, cudaStream_t st, cudaEvent_t* ev) {
-  char* ctrl = ws + P.off_ctrl;
+// the kernels' arguments of one select: plan P over d_keys with the
+// workspace at ws and the control block at ctrl (normally ws + P.off_ctrl)
+static void fill_args(const Plan& P, const void* d_keys, void* d_kth, void* d_vals, int64_t* d_idx, char* ws,
+                      char* ctrl, FusedArgs* out) {
   uint32_t* cw = reinterpret_cast<uint32_t*>(ctrl);
-  if (cudaMemsetAsync(ctrl, 0, P.ctrl_bytes, st) != cudaSuccess) return DRTOPK_ECUDA;
-  if (ev) cudaEventRecord(ev[0], st);
-  if (P.path == PATH_BITONIC) return enqueue_bitonic(P, d_keys, d_kth, d_vals, d_idx, ws, st, ev);
   const bool vec_ok = (reinterpret_cast<uintptr_t>(d_keys) & 15u) == 0;
-  FusedArgs a;
+  FusedArgs& a = *out;
   std::memset(&a, 0, sizeof(a));
   a.keys = static_cast<const uint32_t*>(d_keys);
   a.n = P.n;
@@ -802,6 +851,7 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
   a.tail_flag = cw + CW_TAIL;
   a.pre_hist = cw + P.pre_hist_word;
   a.pre_target = P.pre_target;
+  a.bounded = P.bounded;
   a.phase_lo = 1;
   a.phase_hi = 3;
   a.out_kth = static_cast<uint32_t*>(d_kth);
@@ -838,6 +888,18 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
     a.sort_buf[1] = reinterpret_cast<uint64_t*>(ws + P.off_sort1);
     a.sort_cnt = reinterpret_cast<uint32_t*>(ws + P.off_sortcnt);
   }
+}
+
+drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, void* d_kth, void* d_vals,
+                               int64_t* d_idx, char* ws, cudaStream_t st, cudaEvent_t* ev) {
+  char* ctrl = ws + P.off_ctrl;
+  uint32_t* cw = reinterpret_cast<uint32_t*>(ctrl);
+  if (cudaMemsetAsync(ctrl, 0, P.ctrl_bytes, st) != cudaSuccess) return DRTOPK_ECUDA;
+  if (ev) cudaEventRecord(ev[0], st);
+  if (P.path == PATH_BITONIC) return enqueue_bitonic(P, d_keys, d_kth, d_vals, d_idx, ws, st, ev);
+  const bool vec_ok = (reinterpret_cast<uintptr_t>(d_keys) & 15u) == 0;
+  FusedArgs a;
+  fill_args(P, d_keys, d_kth, d_vals, d_idx, ws, ctrl, &a);
   // ---- sampled-threshold path: sample, predict, emit, then the second select
   if (P.path == PATH_EMIT) {
     if (ev) cudaEventRecord(ev[1], st);
@@ -848,7 +910,9 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
         cudaLaunchKernel(split_ptr(P.km, SK_PRESAMPLE2), dim3(P.presample_grid), dim3(FUSED_THREADS), args, 0, st) !=
             cudaSuccess ||
         cudaLaunchKernel(split_ptr(P.km, SK_EMIT), dim3(P.emit_grid), dim3(FUSED_THREADS), args,
-                         split_smem(P.nb, SK_EMIT), st) != cudaSuccess)
+                         split_smem(P.nb, SK_EMIT), st) != cudaSuccess ||
+        cudaLaunchKernel(split_ptr(P.km, SK_CAND_HIST), dim3(P.hist_grid), dim3(FUSED_THREADS), args,
+                         split_smem(P.nb, SK_CAND_HIST), st) != cudaSuccess)
       s = DRTOPK_ECUDA;
     if (s == DRTOPK_OK) {
       a.split0 = 1;
@@ -860,9 +924,17 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
     if (s == DRTOPK_OK) {
       a.phase_lo = 3;
       a.phase_hi = 3;
-      const int g3 = !P.sorted ? std::min(P.fused_grid, PHASE3_GRID) : P.fused_grid;
-      a.gb.nblocks = (uint32_t)g3;
-      s = launch_coop(fused_ptr(P.km), P, &a, st, g3);
+      if (P.one_cta) {
+        void* args1[] = {&a};
+        a.gb.nblocks = 1;
+        if (cudaLaunchKernel(fused_one_ptr(P.km), dim3(1), dim3(FUSED_THREADS), args1, P.fused_smem, st) !=
+            cudaSuccess)
+          s = DRTOPK_ECUDA;
+      } else {
+        const int g3 = !P.sorted ? std::min(P.fused_grid, PHASE3_GRID) : P.fused_grid;
+        a.gb.nblocks = (uint32_t)g3;
+        s = launch_coop(fused_ptr(P.km), P, &a, st, g3);
+      }
     }
     if (ev) cudaEventRecord(ev[2], st);
     return s;
@@ -947,6 +1019,86 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
   }
   if (ev) cudaEventRecord(ev[2], st);
   return s;
+}
+
+// ------------------------------------------------------------ grouped selects
+// Stages of a grouped sampled-threshold chain, in launch order.
+enum GroupStage : int { GS_PRESAMPLE = 0, GS_PRESAMPLE2, GS_EMIT, GS_CAND_HIST, GS_SPLIT0, GS_LAST, GS_COUNT };
+
+size_t group_desc_bytes(int nprob) {
+  return align256(sizeof(FusedArgs) * (size_t)nprob) + align256(4 * (size_t)GS_COUNT * (nprob + 1));
+}
+
+// CTAs of one select at each stage of a grouped chain, sized to its work
+// (each grouped launch covers every problem of the group)
+static uint32_t group_ctas(const Plan& P, int stage) {
+  const uint64_t n = P.n, k = P.k;
+  const double ks = (double)k / 64.0;
+  const double cand = (double)k + 64.0 * (6.0 * std::sqrt(ks) + 16.0) + (double)n / 65536.0;
+  auto clampc = [](uint64_t v, uint64_t cap) { return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(v, cap)); };
+  switch (stage) {
+    case GS_PRESAMPLE:
+    case GS_PRESAMPLE2: {
+      const uint64_t ns = (n >> 9) / PRE_STRIDE;
+      return clampc((ns + PRE_ROUND * SPLIT_WARPS - 1) / (PRE_ROUND * SPLIT_WARPS), (uint64_t)P.presample_grid);
+    }
+    case GS_EMIT:  // at least eight 512-key chunks per warp
+      return clampc((((n + 511) >> 9) + 8 * SPLIT_WARPS - 1) / (8 * SPLIT_WARPS), (uint64_t)P.emit_grid);
+    case GS_CAND_HIST:
+      return clampc((uint64_t)(1.5 * cand / (FUSED_THREADS * 8)) + 1, (uint64_t)P.hist_grid);
+    case GS_SPLIT0:
+      return clampc((uint64_t)(1.5 * cand / (FUSED_THREADS * 8)) + 1, (uint64_t)P.split0_grid);
+    default:
+      return 1;
+  }
+}
+
+drtopk_status_t enqueue_group(int device, int km, const GroupItem* items, int nprob, char* h_stage, char* d_desc,
+                              uint32_t* d_err_out, cudaStream_t st) {
+  (void)device;
+  if (nprob <= 0) return DRTOPK_OK;
+  FusedArgs* hargs = reinterpret_cast<FusedArgs*>(h_stage);
+  uint32_t* hpre = reinterpret_cast<uint32_t*>(h_stage + align256(sizeof(FusedArgs) * (size_t)nprob));
+  uint32_t tot[GS_COUNT] = {};
+  size_t smem_last = 0;
+  for (int i = 0; i < nprob; ++i) {
+    const Plan& P = *items[i].P;
+    if (P.path != PATH_EMIT || !P.one_cta || P.km != km) return DRTOPK_EINVAL;
+    FusedArgs& a = hargs[i];
+    fill_args(P, items[i].keys, items[i].d_kth, items[i].d_vals, items[i].d_idx, items[i].ws, items[i].ctrl, &a);
+    a.split0 = 1;
+    a.direct0 = P.sorted ? 0 : 1;
+    a.phase_lo = 3;
+    a.phase_hi = 3;
+    a.gb.nblocks = 1;
+    smem_last = std::max(smem_last, P.fused_smem);
+    for (int s = 0; s < GS_COUNT; ++s) {
+      hpre[s * (nprob + 1) + i] = tot[s];
+      tot[s] += group_ctas(P, s);
+    }
+  }
+  for (int s = 0; s < GS_COUNT; ++s) hpre[s * (nprob + 1) + nprob] = tot[s];
+  if (cudaMemcpyAsync(d_desc, h_stage, group_desc_bytes(nprob), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return DRTOPK_ECUDA;
+  const KernelSet& ks = kernels(km);
+  const void* fns[GS_COUNT] = {ks.presample_g, ks.presample2_g, ks.emit_g, ks.cand_hist_g, ks.split0_g,
+                               ks.fused_one_g};
+  const int nb = items[0].P->nb;
+  const size_t smem[GS_COUNT] = {0, 0, split_smem(nb, SK_EMIT), split_smem(nb, SK_CAND_HIST),
+                                 split_smem(nb, SK_SPLIT0), smem_last};
+  if (!fused_one_group_ready(device, km, smem_last)) return DRTOPK_ECUDA;
+  const uint32_t* dpre = reinterpret_cast<const uint32_t*>(d_desc + align256(sizeof(FusedArgs) * (size_t)nprob));
+  for (int s = 0; s < GS_COUNT; ++s) {
+    GroupArgs g;
+    g.probs = reinterpret_cast<const FusedArgs*>(d_desc);
+    g.prefix = dpre + s * (nprob + 1);
+    g.nprob = (uint32_t)nprob;
+    void* args[] = {&g};
+    if (cudaLaunchKernel(fns[s], dim3(tot[s]), dim3(FUSED_THREADS), args, smem[s], st) != cudaSuccess)
+      return DRTOPK_ECUDA;
+  }
+  k_group_errors<<<1, 256, 0, st>>>(reinterpret_cast<const FusedArgs*>(d_desc), (uint32_t)nprob, d_err_out);
+  return cudaGetLastError() == cudaSuccess ? DRTOPK_OK : DRTOPK_ECUDA;
 }
 
 }  // namespace drtopk
@@ -1040,7 +1192,7 @@ extern "C" drtopk_status_t drtopk_sync_check(drtopk_handle_t h, void* stream) {
 
 // kernels one select of plan P launches (enqueue_select's launch sequence)
 static int plan_launches(const Plan& P) {
-  if (P.path == PATH_EMIT) return 5;  // k_presample, k_presample2, k_emit, k_split0, k_fused
+  if (P.path == PATH_EMIT) return 6;  // k_presample, k_presample2, k_emit, k_cand_hist, k_split0, k_fused
   const bool sampler = P.path != PATH_PLAIN && !(P.path == PATH_BITONIC && P.normal);
   int n = sampler ? 1 : 0;
   if (P.path == PATH_BITONIC || P.tail || P.cluster > 0 || !P.split) return n + 1;
@@ -1085,8 +1237,8 @@ extern "C" drtopk_status_t drtopk_last_stats(drtopk_handle_t h, drtopk_stats_t* 
     st->ms_concat = t2 > t1 ? (t2 - t1) * 1e-6 : 0.0;
     st->ms_second = t3 > t2 ? (t3 - t2) * 1e-6 : 0.0;
     st->ms_total = ms_all;
-    st->team_ctas = P.tail ? TAIL_CLUSTER : (P.cluster > 0 ? P.cluster : P.fused_grid);
-    st->team_cluster = P.tail ? 3 : (P.cluster > 0 ? 1 : 0);
+    st->team_ctas = P.tail ? TAIL_CLUSTER : (P.cluster > 0 ? P.cluster : (P.one_cta ? 1 : P.fused_grid));
+    st->team_cluster = P.tail ? 3 : (P.cluster > 0 ? 1 : (P.one_cta ? 5 : 0));
     st->kernel_launches = plan_launches(P);
   }
   cudaSetDevice(cur);

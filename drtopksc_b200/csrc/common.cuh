@@ -248,6 +248,7 @@ enum DevErr : uint32_t {
   DE_BARRIER_TIMEOUT = 1u,   // a grid barrier gave up waiting
   DE_OVERFLOW = 2u,          // a bounded buffer would have overflowed (skipped)
   DE_INTERNAL = 4u,          // an invariant failed (result not trusted)
+  DE_RETRY = 8u,             // a bounded select could not finish in its workspace: run it with the general plan
 };
 
 // Grid barrier for kernels launched cooperatively (all CTAs co-resident).

@@ -741,6 +741,18 @@ DRTOPK_DEV Level cand_level0(uint32_t thr, int nbits, uint32_t R) {
   return L;
 }
 
+// Level 0 over candidates known to lie in [thr, mx]: the same power-of-two
+// radix bins, cut to the candidates' span (keys that crowd just above the
+// threshold -- float keys, narrow distributions -- spread over the bins
+// instead of landing in the first few)
+DRTOPK_DEV Level cand_level0_tight(uint32_t thr, uint32_t mx, int nbits, uint32_t R) {
+  Level L;
+  const uint32_t top = mx - thr;
+  const int bits = 32 - __clz(top);
+  L.lo = thr; L.hi = mx; L.wshift = max(0, bits - nbits); L.w = 1u << L.wshift; L.R = R;
+  return L;
+}
+
 DRTOPK_DEV Level bucket_level0(uint32_t mn, uint32_t mx, int nb, uint32_t R) {
   Level L;
   L.lo = mn; L.hi = mx; L.wshift = -1;

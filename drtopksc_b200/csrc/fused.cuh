@@ -73,6 +73,7 @@ struct FusedArgs {
   int direct0;            // ... writing its top entries straight to the (unsorted) output
   uint32_t* pre_hist;     // [2][256] sampled-threshold path: top / second byte counts of the key sample
   uint32_t pre_target;    // sampled keys that must lie at or above the predicted threshold
+  int bounded;            // candidate buffers sized by the sample's estimate: no device fallback
   GridBar gb;
 };
 
@@ -481,6 +482,12 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
   // threshold means the prediction overshot the k-th key; the select then
   // runs over all keys (plain radix), so the answer stays exact
   const bool emit_fb = a.path == PATH_EMIT && (ld_cg_u32(a.cand_count) < a.k || ld_cg_u32(a.cand_count) > a.cand_cap);
+  if (emit_fb && a.bounded) {
+    // buffers sized by the estimate cannot hold the general select: the
+    // caller runs this request again with its general plan
+    if (lead) atomicOr(a.gb.err, (uint32_t)DE_RETRY);
+    return;
+  }
   if (emit_fb) {
     zero_words(tm, a.C.H[0], a.nb);
     if (!team_sync(tm)) return;
@@ -509,7 +516,10 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
   } else {
     // candidates of the sampled paths are all >= thr1 (their level-0
     // histogram was built against this level by the concatenation)
-    L0c = (a.path == PATH_PLAIN || emit_fb) ? radix_level0(a.nbits, a.k) : cand_level0(thr1, a.nbits, a.k);
+    L0c = (a.path == PATH_PLAIN || emit_fb)
+              ? radix_level0(a.nbits, a.k)
+              : (a.path == PATH_EMIT ? cand_level0_tight(thr1, ld_cg_u32(a.cand_minmax + 1), a.nbits, a.k)
+                                     : cand_level0(thr1, a.nbits, a.k));
   }
   EngineCfg cc;
   cc.bucket = a.bucket; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
@@ -586,6 +596,19 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_fused(FusedArgs a) {
   fused_body<KM>(a, grid_team(a.gb), s_dyn);
 }
 
+// one ordinary CTA is the team: no co-residency with other CTAs is needed, so
+// the launch never waits for a share of the GPU and overlaps other streams'
+// kernels (the served form's last levels of a sampled-threshold select)
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_fused_one(FusedArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  Team t = {};
+  t.rank = 0;
+  t.size = 1;
+  t.cluster = 2;
+  fused_body<KM>(a, t, s_dyn);
+}
+
 // cluster launch: every thread-block cluster is the team of one problem --
 // problem clusterid.x of `list`, or the kernel argument when list is null
 template <int KM>
@@ -650,6 +673,7 @@ struct CandStage {
   int cs;
   uint32_t mlo, mhi;
   bool ovf;
+  bool track_max;  // record the largest key instead of the level-0 histogram
 
   DRTOPK_DEV void drain(const FusedArgs& a, uint32_t* s_hist) {
     __syncwarp();
@@ -662,7 +686,8 @@ struct CandStage {
       const uint2 v = buf[i];
       if ((uint64_t)base + i < a.cand_cap) a.cand[base + i] = v;
       else ovf = true;
-      if (a.bucket) { mlo = max(mlo, ~v.x); mhi = max(mhi, v.x); }
+      if (track_max) mhi = max(mhi, v.x);
+      else if (a.bucket) { mlo = max(mlo, ~v.x); mhi = max(mhi, v.x); }
       else hist_add_warp(s_hist, (v.x - thr) >> cs);
     }
     __syncwarp();
@@ -782,8 +807,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_level_hist(FusedArgs a) {
 constexpr int SPLIT0_E = 8;  // entries per thread per tile (register budget of 4 CTAs / SM)
 
 template <int KM>
-__global__ void __launch_bounds__(FUSED_THREADS, 4) k_split0(FusedArgs a) {
-  extern __shared__ __align__(16) uint32_t s_dyn[];
+DRTOPK_DEV void split0_body(const FusedArgs& a, uint32_t cta, uint32_t ncta, uint32_t* s_dyn) {
   uint32_t* s_hist = s_dyn;
   const uint32_t thr = ld_cg_u32(a.thr_word);
   const uint32_t ncand = ld_cg_u32(a.cand_count);
@@ -791,7 +815,8 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_split0(FusedArgs a) {
   EngineCfg cc;
   cc.bucket = 0; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
   cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0; cc.skip_split0 = 0;
-  const Level L0 = cand_level0(thr, a.nbits, a.k);
+  const Level L0 = a.path == PATH_EMIT ? cand_level0_tight(thr, ld_cg_u32(a.cand_minmax + 1), a.nbits, a.k)
+                                       : cand_level0(thr, a.nbits, a.k);
   const Pick p = block_pick<false>(a.C.H[0], a.nb, L0.R);
   Level N;
   const bool done = advance(cc, L0, p, 0, N);
@@ -799,7 +824,9 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_split0(FusedArgs a) {
   Src sc = {};
   sc.pairs = a.cand;
   sc.count_dev = a.cand_count;
-  const Team tm = grid_team(a.gb);
+  Team tm = grid_team(a.gb);
+  tm.rank = cta;
+  tm.size = ncta;
   if (a.direct0)
     split_tiles<KM, true, SPLIT0_E>(tm, cc, sc, true, ncand, N, !done, a.C, a.C.top_count, a.C.cbuf[0], a.C.set_count + 1,
                           s_hist, a.C.top_cap, a.C.cbuf_cap, a.C.err);
@@ -807,6 +834,12 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_split0(FusedArgs a) {
     split_tiles<KM, false, SPLIT0_E>(tm, cc, sc, true, ncand, N, !done, a.C, a.C.top_count, a.C.cbuf[0], a.C.set_count + 1,
                            s_hist, a.C.top_cap, a.C.cbuf_cap, a.C.err);
   if (!done) flush_hist(s_hist, a.C.H[1], a.nb);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_split0(FusedArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  split0_body<KM>(a, blockIdx.x, gridDim.x, s_dyn);
 }
 
 // Beta filter (FindTopKRanges_beta, radixselect.cuh:560-598) over batches of
@@ -837,7 +870,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_filter(FusedArgs a) {
     thr = ld_cg_u32(a.thr_word);
   }
   clear_hist(s_hist, a.nb);
-  CandStage cst = {cstage, (uint32_t)SPLIT_STAGE, 0u, thr, cand_shift(thr, a.nbits), 0u, 0u, false};
+  CandStage cst = {cstage, (uint32_t)SPLIT_STAGE, 0u, thr, cand_shift(thr, a.nbits), 0u, 0u, false, false};
   uint32_t ns = 0;               // staged selected ids (warp-uniform)
   uint32_t nsel = 0, nlone = 0;  // this warp's totals
   auto drain_sel = [&]() {
@@ -941,7 +974,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_gather(FusedArgs a) {
     ids1 = a.sel;
   }
   clear_hist(s_hist, a.nb);
-  CandStage cst = {cstage, (uint32_t)GATHER_STAGE, 0u, thr, cand_shift(thr, a.nbits), 0u, 0u, false};
+  CandStage cst = {cstage, (uint32_t)GATHER_STAGE, 0u, thr, cand_shift(thr, a.nbits), 0u, 0u, false, false};
   // granule and key indices fit 32 bits (n < 2^32); only the round counter
   // is 64-bit
   const int alpha = a.alpha;
@@ -1064,13 +1097,14 @@ DRTOPK_DEV void chunk_keys(const FusedArgs& a, uint64_t ch, uint64_t pol, uint32
 }
 
 template <int KM>
-DRTOPK_DEV void presample_pass(const FusedArgs& a, int level, uint32_t b0, uint32_t (*s_h)[256]) {
+DRTOPK_DEV void presample_pass(const FusedArgs& a, int level, uint32_t b0, uint32_t (*s_h)[256], uint32_t cta,
+                               uint32_t ncta) {
   const unsigned lane = lane_id();
   const int wib = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < SPLIT_WARPS * 256; i += blockDim.x) (&s_h[0][0])[i] = 0;
   __syncthreads();
   const uint64_t ns = (a.n >> 9) / PRE_STRIDE;
-  const uint64_t gw = (uint64_t)blockIdx.x * SPLIT_WARPS + wib, nw = (uint64_t)gridDim.x * SPLIT_WARPS;
+  const uint64_t gw = (uint64_t)cta * SPLIT_WARPS + wib, nw = (uint64_t)ncta * SPLIT_WARPS;
   // PRE_ROUND sampled chunks per warp and round, all loaded before any is
   // counted (the pass is latency-bound); a small persistent grid keeps the
   // histogram flushes few
@@ -1115,46 +1149,52 @@ DRTOPK_DEV void presample_pass(const FusedArgs& a, int level, uint32_t b0, uint3
 }
 
 template <int KM>
-__global__ void __launch_bounds__(FUSED_THREADS) k_presample(FusedArgs a) {
+DRTOPK_DEV void presample_body(const FusedArgs& a, uint32_t cta, uint32_t ncta) {
   __shared__ uint32_t s_h[SPLIT_WARPS][256];
-  if (blockIdx.x == 0 && threadIdx.x == 0) stamp(a.stats, 16);
-  presample_pass<KM>(a, 0, 0u, s_h);
+  if (cta == 0 && threadIdx.x == 0) stamp(a.stats, 16);
+  presample_pass<KM>(a, 0, 0u, s_h, cta, ncta);
+}
+
+template <int KM>
+DRTOPK_DEV void presample2_body(const FusedArgs& a, uint32_t cta, uint32_t ncta) {
+  __shared__ uint32_t s_h2[SPLIT_WARPS][256];
+  const Pick p0 = block_pick<false>(a.pre_hist, 256, a.pre_target);
+  presample_pass<KM>(a, 1, (uint32_t)p0.b, s_h2, cta, ncta);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_presample(FusedArgs a) {
+  presample_body<KM>(a, blockIdx.x, gridDim.x);
 }
 
 template <int KM>
 __global__ void __launch_bounds__(FUSED_THREADS) k_presample2(FusedArgs a) {
-  __shared__ uint32_t s_h[SPLIT_WARPS][256];
-  const Pick p0 = block_pick<false>(a.pre_hist, 256, a.pre_target);
-  presample_pass<KM>(a, 1, (uint32_t)p0.b, s_h);
+  presample2_body<KM>(a, blockIdx.x, gridDim.x);
 }
 
 template <int KM>
-__global__ void __launch_bounds__(FUSED_THREADS, 4) k_emit(FusedArgs a) {
-  extern __shared__ __align__(16) uint32_t s_dyn[];
-  // one histogram copy per warp (candidates crowd into a few bins), summed
-  // before the flush
-  const int hw = split_hist_words(a.nb);
+DRTOPK_DEV void emit_body(const FusedArgs& a, uint32_t cta, uint32_t ncta, uint32_t* s_dyn) {
   const unsigned lane = lane_id();
   const int wib = threadIdx.x >> 5;
-  uint32_t* s_hist = s_dyn + (size_t)wib * hw;
-  uint2* cstage = reinterpret_cast<uint2*>(s_dyn + (size_t)SPLIT_WARPS * hw) + (size_t)wib * GATHER_STAGE;
+  uint2* cstage = reinterpret_cast<uint2*>(s_dyn) + (size_t)wib * GATHER_STAGE;
   // the predicted threshold: 16-bit prefix boundary holding pre_target
   // sampled keys at or above it
   const Pick p0 = block_pick<false>(a.pre_hist, 256, a.pre_target);
   const uint32_t r1 = a.pre_target > p0.above ? a.pre_target - p0.above : 1u;
   const Pick p1 = block_pick<false>(a.pre_hist + 256, 256, r1);
   const uint32_t thr = ((uint32_t)p0.b << 24) | ((uint32_t)p1.b << 16);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (cta == 0 && threadIdx.x == 0) {
     *a.thr_word = thr;
     a.stats[ST_LVA] = 2;
     stamp(a.stats, 18);
   }
-  for (int i = threadIdx.x; i < SPLIT_WARPS * hw; i += blockDim.x) s_dyn[i] = 0;
-  __syncthreads();
-  CandStage cst = {cstage, (uint32_t)GATHER_STAGE, 0u, thr, cand_shift(thr, a.nbits), 0u, 0u, false};
+  // the candidates' largest key bounds level 0 of the second select
+  // (k_cand_hist builds its histogram once the span is known)
+  CandStage cst = {cstage, (uint32_t)GATHER_STAGE, 0u, thr, 0, 0u, 0u, false, true};
+  uint32_t* s_hist = nullptr;
   const uint64_t pol = make_evict_first_policy();
   const uint64_t nchunks = (a.n + 511) >> 9;
-  const uint64_t gw = (uint64_t)blockIdx.x * SPLIT_WARPS + wib, nw = (uint64_t)gridDim.x * SPLIT_WARPS;
+  const uint64_t gw = (uint64_t)cta * SPLIT_WARPS + wib, nw = (uint64_t)ncta * SPLIT_WARPS;
   // register double buffer: the next chunk's loads are in flight while this
   // chunk is compared and compacted
   uint32_t kn[4][4];
@@ -1207,13 +1247,147 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_emit(FusedArgs a) {
   }
   cst.drain(a, s_hist);
   if (cst.ovf) atomicOr(a.gb.err, (uint32_t)DE_OVERFLOW);
-  __syncthreads();
-  for (int b = threadIdx.x; b < a.nb; b += blockDim.x) {
-    uint32_t c = 0;
+  uint32_t mx = cst.mhi;
 #pragma unroll
-    for (int w = 0; w < SPLIT_WARPS; ++w) c += s_dyn[(size_t)w * hw + b];
-    if (c) atomicAdd(&a.C.H[0][b], c);
+  for (int off = 16; off > 0; off >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  if (lane == 0 && mx) atomicMax(&a.cand_minmax[1], mx);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_emit(FusedArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  emit_body<KM>(a, blockIdx.x, gridDim.x, s_dyn);
+}
+
+// Level-0 histogram of the sampled-threshold path's candidates over
+// [thr, largest candidate] (cand_level0_tight), for k_split0's pick
+template <int KM>
+DRTOPK_DEV void cand_hist_body(const FusedArgs& a, uint32_t cta, uint32_t ncta, uint32_t* s_dyn) {
+  uint32_t* s_hist = s_dyn;
+  const uint32_t thr = ld_cg_u32(a.thr_word);
+  const uint32_t ncand = ld_cg_u32(a.cand_count);
+  if (ncand < a.k || ncand > a.cand_cap) return;  // uniform: the last kernel falls back
+  const Level L0 = cand_level0_tight(thr, ld_cg_u32(a.cand_minmax + 1), a.nbits, a.k);
+  clear_hist(s_hist, a.nb);
+  const uint64_t T = (uint64_t)blockDim.x * 8;
+  for (uint64_t tb = (uint64_t)cta * T; tb < ncand; tb += (uint64_t)ncta * T) {
+    uint32_t v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const uint64_t i = tb + (uint64_t)u * blockDim.x + threadIdx.x;
+      v[u] = i < ncand ? ld_cg_u32(reinterpret_cast<const uint32_t*>(a.cand + i)) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const bool in = tb + (uint64_t)u * blockDim.x + threadIdx.x < ncand;
+      hist_add_conv(s_hist, in, bin_of(v[u], L0.lo, L0.w, L0.wshift));
+    }
   }
+  flush_hist(s_hist, a.C.H[0], a.nb);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_cand_hist(FusedArgs a) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  cand_hist_body<KM>(a, blockIdx.x, gridDim.x, s_dyn);
+}
+
+// ---------------------------------------------------------------- grouped launches
+// The served form runs the sampled-threshold selects admitted together as
+// one chain of launches: every kernel covers all problems of a group (one
+// key mode), each problem getting the CTAs a prefix table assigns it, and
+// the last levels run one CTA per problem.  A CTA finds its problem by
+// binary search in the prefix (cta_prefix[p] <= blockIdx.x <
+// cta_prefix[p+1]) and copies the problem's arguments into shared memory.
+struct GroupArgs {
+  const FusedArgs* probs;
+  const uint32_t* prefix;  // [nprob + 1] CTA prefix of this launch
+  uint32_t nprob;
+};
+
+DRTOPK_DEV const FusedArgs& group_problem(const GroupArgs& g, FusedArgs* s_args, uint32_t& cta, uint32_t& ncta) {
+  __shared__ uint32_t s_p;
+  if (threadIdx.x == 0) {
+    uint32_t lo = 0, hi = g.nprob;  // largest p with prefix[p] <= blockIdx.x
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(g.prefix + mid) <= blockIdx.x) lo = mid;
+      else hi = mid;
+    }
+    s_p = lo;
+  }
+  __syncthreads();
+  const uint32_t p = s_p;
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(g.probs + p);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(s_args);
+  for (int i = threadIdx.x; i < (int)(sizeof(FusedArgs) / 4); i += blockDim.x) dst[i] = __ldg(src + i);
+  cta = blockIdx.x - __ldg(g.prefix + p);
+  ncta = __ldg(g.prefix + p + 1) - __ldg(g.prefix + p);
+  __syncthreads();
+  return *s_args;
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_presample_g(GroupArgs g) {
+  __shared__ FusedArgs s_args;
+  uint32_t cta, ncta;
+  const FusedArgs& a = group_problem(g, &s_args, cta, ncta);
+  presample_body<KM>(a, cta, ncta);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_presample2_g(GroupArgs g) {
+  __shared__ FusedArgs s_args;
+  uint32_t cta, ncta;
+  const FusedArgs& a = group_problem(g, &s_args, cta, ncta);
+  presample2_body<KM>(a, cta, ncta);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_emit_g(GroupArgs g) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  __shared__ FusedArgs s_args;
+  uint32_t cta, ncta;
+  const FusedArgs& a = group_problem(g, &s_args, cta, ncta);
+  emit_body<KM>(a, cta, ncta, s_dyn);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_cand_hist_g(GroupArgs g) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  __shared__ FusedArgs s_args;
+  uint32_t cta, ncta;
+  const FusedArgs& a = group_problem(g, &s_args, cta, ncta);
+  cand_hist_body<KM>(a, cta, ncta, s_dyn);
+}
+
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS, 4) k_split0_g(GroupArgs g) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  __shared__ FusedArgs s_args;
+  uint32_t cta, ncta;
+  const FusedArgs& a = group_problem(g, &s_args, cta, ncta);
+  split0_body<KM>(a, cta, ncta, s_dyn);
+}
+
+// the device error word of every problem of a group, gathered for one copy
+// back (the served form retries problems flagged DE_RETRY)
+static __global__ void k_group_errors(const FusedArgs* probs, uint32_t nprob, uint32_t* out) {
+  for (uint32_t i = threadIdx.x; i < nprob; i += blockDim.x) out[i] = ld_cg_u32(probs[i].gb.err);
+}
+
+// the last levels: CTA p runs problem p alone
+template <int KM>
+__global__ void __launch_bounds__(FUSED_THREADS) k_fused_one_g(GroupArgs g) {
+  extern __shared__ __align__(16) uint32_t s_dyn[];
+  __shared__ FusedArgs s_args;
+  uint32_t cta, ncta;
+  const FusedArgs& a = group_problem(g, &s_args, cta, ncta);
+  Team t = {};
+  t.rank = 0;
+  t.size = 1;
+  t.cluster = 2;
+  fused_body<KM>(a, t, s_dyn);
 }
 
 }  // namespace drtopk

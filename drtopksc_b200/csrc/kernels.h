@@ -9,6 +9,7 @@ namespace drtopk {
 struct KernelSet {
   const void* fused;       // k_fused<KM>
   const void* fused_cl;    // k_fused_cl<KM>
+  const void* fused_one;   // k_fused_one<KM>
   const void* tail;        // k_tail<KM>
   const void* filter;      // k_filter<KM>
   const void* gather;      // k_gather<KM>
@@ -18,6 +19,14 @@ struct KernelSet {
   const void* presample;   // k_presample<KM>   (sampled-threshold path)
   const void* presample2;  // k_presample2<KM>
   const void* emit;        // k_emit<KM>
+  const void* cand_hist;   // k_cand_hist<KM>
+  // grouped forms of the sampled-threshold path (many problems per launch)
+  const void* presample_g;
+  const void* presample2_g;
+  const void* emit_g;
+  const void* cand_hist_g;
+  const void* split0_g;
+  const void* fused_one_g;
   const void* sample1;     // k_sample<KM, 1, false, false>  (alpha <= 8)
   const void* sample2;     // k_sample<KM, 2, false, false>
   const void* sample2pos;  // k_sample<KM, 2, true, false>

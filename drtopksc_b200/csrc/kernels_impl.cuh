@@ -15,6 +15,7 @@ KernelSet make_kernel_set() {
   KernelSet s;
   s.fused = (const void*)k_fused<KM>;
   s.fused_cl = (const void*)k_fused_cl<KM>;
+  s.fused_one = (const void*)k_fused_one<KM>;
   s.tail = (const void*)k_tail<KM>;
   s.filter = (const void*)k_filter<KM>;
   s.gather = (const void*)k_gather<KM>;
@@ -24,6 +25,13 @@ KernelSet make_kernel_set() {
   s.presample = (const void*)k_presample<KM>;
   s.presample2 = (const void*)k_presample2<KM>;
   s.emit = (const void*)k_emit<KM>;
+  s.cand_hist = (const void*)k_cand_hist<KM>;
+  s.presample_g = (const void*)k_presample_g<KM>;
+  s.presample2_g = (const void*)k_presample2_g<KM>;
+  s.emit_g = (const void*)k_emit_g<KM>;
+  s.cand_hist_g = (const void*)k_cand_hist_g<KM>;
+  s.split0_g = (const void*)k_split0_g<KM>;
+  s.fused_one_g = (const void*)k_fused_one_g<KM>;
   s.sample1 = (const void*)k_sample<KM, 1, false, false>;
   s.sample2 = (const void*)k_sample<KM, 2, false, false>;
   s.sample2pos = (const void*)k_sample<KM, 2, true, false>;

@@ -40,6 +40,9 @@ struct Plan {
   int split;           // concatenation as separate kernels (large inputs)
   int cluster;         // > 0: phases after the sampler run in one thread-block cluster of this many CTAs
   int tail;            // 1: phases after the sampler run in one CTA with the sets in shared memory
+  int one_cta;         // sampled-threshold path: the last levels run in one ordinary CTA (no co-residency)
+  int bounded;         // ... with candidate buffers of cap_bound entries (served form; DE_RETRY on overflow)
+  uint64_t cap_bound;
   int split_grid, filter_grid, hist_grid, split0_grid;
   int emit_grid, presample_grid;  // sampled-threshold path
   uint32_t pre_target;            // sampled keys required at or above its predicted threshold
@@ -65,9 +68,37 @@ drtopk_status_t make_plan(uint64_t n, uint64_t k, drtopk_dtype_t dtype, const dr
 void layout(Plan* P, bool want_idx);
 drtopk_status_t plan_select(int device, uint64_t n, uint64_t k, drtopk_dtype_t dtype, const drtopk_params_t* p,
                             bool want_idx, Plan* P);
+// Served form: as plan_select; a sampled-threshold plan with one-CTA last
+// levels gets candidate buffers sized by the sample's estimate (bounded):
+// such a select that cannot finish in them reports DE_RETRY instead of
+// falling back on the device, and its caller runs it with a general plan.
+drtopk_status_t plan_select_bounded(int device, uint64_t n, uint64_t k, drtopk_dtype_t dtype,
+                                    const drtopk_params_t* p, bool want_idx, Plan* P);
 drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, void* d_kth, void* d_vals,
                                int64_t* d_idx, char* ws, cudaStream_t st, cudaEvent_t* ev);
 int ref_alpha(double log2n, double k);
+
+// One select of a grouped launch (sampled-threshold plans with one_cta set,
+// one key mode per group): its plan, input, outputs, workspace and its
+// control block (zeroed by the caller before enqueue_group).
+struct GroupItem {
+  const Plan* P;
+  const void* keys;
+  void* d_kth;
+  void* d_vals;
+  int64_t* d_idx;
+  char* ws;
+  char* ctrl;
+};
+// bytes of the device descriptor area enqueue_group needs for nprob selects
+// (and of the pinned host staging it fills)
+size_t group_desc_bytes(int nprob);
+// Enqueue nprob selects as one chain of grouped launches on st.  h_stage is
+// pinned host memory and d_desc device memory, both group_desc_bytes(nprob)
+// bytes; h_stage must stay untouched until the upload has run.  Every
+// problem's device error word ends up in d_err_out[nprob].
+drtopk_status_t enqueue_group(int device, int km, const GroupItem* items, int nprob, char* h_stage, char* d_desc,
+                              uint32_t* d_err_out, cudaStream_t st);
 // status of a device error word: 0 -> OK, a bounded wait that gave up ->
 // ETIMEOUT, any other device-side check -> EDEVICE
 drtopk_status_t device_error_status(uint32_t err);

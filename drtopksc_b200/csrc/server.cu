@@ -2,26 +2,23 @@
 //
 // A worker thread admits queued requests as in-flight slots and the HBM byte
 // budget allow, and keeps admitting while earlier requests are still on the
-// GPU:
-//   * requests with n <= 2^22 and k <= 4096 admitted in the same tick are
-//     grouped into ONE persistent segmented launch (segmented.cuh), each
-//     segment reading and writing its request's own buffers;
-//   * other requests run one select each: in order on the select stream
-//     (the whole-GPU cooperative tail: one at a time), or on a stream of
-//     their own when their tail is the one-CTA shared-memory kernel, which
-//     then overlaps the other streams' work;
-//   * each request's outputs come back with ONE device-to-host copy on the
-//     copy stream paired with its compute stream, ordered after its kernels
-//     by an event, so result copies never stall the compute streams.
-// Device memory: a request's keys copy and workspace come from the
-// stream-ordered pool and go back on the same compute stream right after its
-// kernels; its outputs come from a per-server cache and go back when its
-// completion event has fired.  The worker holds the server mutex only to
-// move requests between the queue, the admitted set and the result list;
-// CUDA calls run unlocked.
-// Results are exact and identical to the plain call (same kernels / same
-// integer arithmetic); results are copied into the caller's host buffers
-// before poll() reports them.
+// GPU.  The requests admitted in one tick become, per key mode, ONE chain of
+// grouped launches of the sampled-threshold select (enqueue_group): every
+// launch covers all of the chain's problems, each problem getting the CTAs
+// its size calls for, and the last levels run one CTA per problem -- no
+// launch needs the whole GPU, so chains on different streams overlap.  A
+// chain's control blocks, workspaces (candidate buffers sized by the key
+// sample's estimate), host-mode keys and outputs live in one stream-ordered
+// arena; its outputs come back with one device-to-host copy.  A select whose
+// sample misjudged the input (DE_RETRY) runs again on the completion thread
+// with the general plan.  Sorted requests of more than 4096 keys keep the
+// whole-GPU sort and run one at a time on their own stream.
+// Host time per request is its share of one chain's launches, which is what
+// lets the server outrun a loop of plain calls.  The completion thread polls
+// the chains' events, copies results into the callers' buffers and publishes
+// them; neither thread holds the server mutex during CUDA calls.
+// Results are exact and identical to the plain call (same integer
+// arithmetic).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,7 +37,7 @@
 
 #include "../../include/drtopk.h"
 #include "plan.h"
-#include "segmented.cuh"
+#include "fused.cuh"
 
 using namespace drtopk;
 
@@ -49,24 +46,28 @@ namespace {
 // stream roles: compute streams, each paired with its own copy stream for
 // the result copies and completion events (a request's copy waits only for
 // its own stream's kernels, never behind another stream's slower request)
-constexpr int ST_BATCH = 0;    // micro-batches (segmented kernel, not cooperative)
+constexpr int ST_AUX = 0;      // server set-up work (memory pool warm-up)
 constexpr int ST_TAIL = 1;     // single selects with the one-CTA shared-memory tail
 constexpr int ST_SINGLE = 2;   // first of NSINGLE streams for the other single selects (dealt
                                // round-robin when NSINGLE > 1)
-// Single selects run in order on one stream with the planner's own team
-// choice (the whole-GPU cooperative tail for large problems: one at a time).
-// Four streams with the shared-GPU team (SINGLE_TEAM 4: each tail in one
-// 8-CTA cluster, overlapping the other streams' samplers) reached 14-17 K
-// req/s on the bench mix against ~11.5 K, but under saturation a cluster
-// launch could wait seconds for 8 free SMs of one GPC while the other
-// streams' samplers kept arriving (p99 1.7-2.7 s, 0.7-1.2 K req/s in two
-// runs), so it is not the default.
-constexpr int NSINGLE = 1;
+// Single selects take the sampled-threshold path with every launch an
+// ordinary one (sample passes, the appending pass and the level-0 split over
+// the whole GPU, the last levels in one CTA, team 5): no launch waits for a
+// share of the GPU, so the selects of NSINGLE - 1 streams overlap, one's
+// streaming filling the SMs another's last levels leave free.  Cooperative
+// or cluster tails on several streams starve under load (a cluster launch
+// waited seconds for 8 free SMs of one GPC while other streams' samplers
+// kept arriving), so the one kind of single that keeps a cooperative kernel
+// -- sorted output of more than SINGLE_ONE_CTA_SORT_K keys, sorted over the
+// whole GPU -- runs in order on the first single stream.
+constexpr int NSINGLE = 8;
 constexpr int SINGLE_TEAM = 0;
 constexpr int NCOMPUTE = ST_SINGLE + NSINGLE;
 constexpr int ST_COPY = NCOMPUTE;  // copy stream of compute stream i: ST_COPY + i
 constexpr int NSTREAMS = 2 * NCOMPUTE;
-constexpr uint64_t BATCH_MAX_N = 1ull << 22;  // larger inputs run as single selects
+constexpr uint64_t SINGLE_ONE_CTA_SORT_K = 4096;     // sorted outputs larger than this keep the whole-GPU sort
+constexpr size_t GROUP_OUT_CAP = size_t(32) << 20;   // output bytes of one grouped launch chain
+constexpr size_t PREWARM_POOL = size_t(8) << 30;     // device pool bytes mapped at server creation
 
 struct Req {
   uint64_t id = 0;
@@ -99,9 +100,9 @@ struct Req {
   drtopk_result_t res = {};
   double t_submit = 0, t_start = 0, t_done = 0;
   int status = DRTOPK_OK;
-  bool small = false;
   bool planned = false;              // plan computed once, at first admission attempt
   Plan plan;
+  const uint32_t* errp = nullptr;    // grouped: the device error word, in the group's staging
 };
 
 // Process-wide cache of pinned host buffers (size classes of powers of two),
@@ -138,7 +139,7 @@ struct PinnedCache {
     return p;
   }
   void put(void* p, size_t cap) {
-    if (!p) return;
+    if (!p || cap == 0) return;  // cap 0: a view into a buffer another request owns
     std::lock_guard<std::mutex> lk(mu);
     if (cached + cap > (size_t(8) << 30)) {
       cudaFreeHost(p);
@@ -210,8 +211,6 @@ struct drtopk_server {
   cudaStream_t streams[NSTREAMS] = {};
   uint64_t next_single = 0;  // round-robin over the single-select streams (worker thread only)
   cudaEvent_t ev_kernels = nullptr;  // kernels-done marker (re-recorded per launch)
-  int seg_grid = 0;
-  size_t seg_smem = 0;
   std::mutex mu;
   std::condition_variable cv, done_cv;
   std::deque<Req*> queue;           // guarded by mu
@@ -253,7 +252,7 @@ struct drtopk_server {
     size_t b = 0;
     if (!r->dkeys_user) b += al256(r->n * 4);
     b += al256(4) + al256(r->k * 4) + al256(r->k * 8);
-    if (!r->small) {
+    {
       // the request's one plan: autotuned parameters, SINGLE_TEAM
       if (!r->planned) {
         drtopk_params_t p;
@@ -261,15 +260,20 @@ struct drtopk_server {
         p.alpha = -2;
         p.sorted = r->sorted;
         p.team = SINGLE_TEAM;
-        drtopk_status_t s = plan_select(device, r->n, r->k, r->dtype, &p, r->user_idx != nullptr, &r->plan);
+        if (!r->sorted || r->k <= SINGLE_ONE_CTA_SORT_K) {
+          // the sampled-threshold path with every launch an ordinary one (the
+          // last levels in one CTA): no launch waits for a share of the GPU,
+          // so the single streams' selects overlap
+          p.alpha = 0;
+          p.path = 4;
+          p.team = 5;
+        }
+        drtopk_status_t s = plan_select_bounded(device, r->n, r->k, r->dtype, &p, r->user_idx != nullptr, &r->plan);
         if (s != DRTOPK_OK) return s;
         r->planned = true;
       }
       r->ws_bytes = r->plan.ws_bytes;
       b += al256(r->ws_bytes);
-    } else {
-      // share of the batch workspace: delegates + candidates of its segment
-      b += al256(r->n / 16 * 4) + al256(r->k * 8 * 256);
     }
     *out = b;
     return DRTOPK_OK;
@@ -282,7 +286,14 @@ struct drtopk_server {
   void launch_admitted(std::vector<Req*>& v);
   void complete_loop();
   void launch_single(Req* r);
-  void launch_batch(std::vector<Req*>& v, int si);
+  void launch_group(std::vector<Req*>& v, int si);
+  void prewarm();
+  void retry_general(Req* r);
+  void retry_general_run(Req* r);
+  drtopk_handle_t h_retry = nullptr;  // completion thread only
+  double alloc_ms = 0;                // worker thread: time in cudaMallocAsync (read under mu via stats)
+  uint64_t retries = 0;               // completion thread
+  double retry_ms = 0;
   void loop();
 };
 
@@ -362,107 +373,154 @@ void drtopk_server::launch_single(Req* r) {
   finish_on_copy_stream(r, ev_kernels);
 }
 
-void drtopk_server::launch_batch(std::vector<Req*>& v, int si) {
+// Sampled-threshold singles of one key mode admitted in the same tick: one
+// device arena (control blocks, workspaces, host-mode keys, outputs, launch
+// descriptors), one chain of grouped launches (enqueue_group), one copy of
+// all outputs back, one free.  Host work per request drops to filling its
+// descriptor; the grouped kernels keep the GPU busy across problems.
+void drtopk_server::launch_group(std::vector<Req*>& v, int si) {
   cudaStream_t st = streams[si];
-  const int nseg = (int)v.size();
-  std::vector<SegDesc> seg(nseg);
-  std::vector<uint2> tasks;
-  uint64_t del_total = 0, cand_total = 0;
-  for (int s = 0; s < nseg; ++s) {
-    Req* r = v[s];
-    r->stream = si;
-    SegDesc& d = seg[s];
-    std::memset(&d, 0, sizeof(d));
-    d.len = (uint32_t)r->n;
-    d.k = (uint32_t)r->k;
-    d.km = r->dtype == DRTOPK_F32 ? KM_F32 : KM_U32;
-    d.kptr = r->dkeys_user ? static_cast<const uint32_t*>(r->dkeys_user) : r->d_keys;
-    d.okth = r->d_kth;
-    d.ovals = r->d_vals;
-    d.oidx = r->user_idx ? r->d_idx : nullptr;
-    d.sorted = r->sorted;
-    // same per-segment choice as the batched form
-    if (d.len <= 32768) {
-      d.mode = SEG_PLAIN;
-    } else {
-      int a = (int)std::lround(std::log2(std::max(2.0, std::sqrt(5.0 * d.len / d.k))));
-      a = std::max(5, std::min(a, 15));
-      while (a > 5 && ((((uint64_t)d.len + (1ull << a) - 1) >> a) < d.k)) a--;
-      if ((((uint64_t)d.len + (1ull << a) - 1) >> a) < d.k) {
-        d.mode = SEG_PLAIN;
-      } else {
-        d.mode = SEG_DELEGATE;
-        d.alpha = a;
-      }
-    }
-    if (d.mode == SEG_DELEGATE) {
-      const uint64_t S = 1ull << d.alpha, M = (d.len + S - 1) >> d.alpha;
-      d.del_off = del_total;
-      del_total += M;
-      d.cand_off = cand_total;
-      cand_total += (uint64_t)d.k * S;
-      d.ntasks = (int)((d.len + SEG_CH - 1) / SEG_CH);
-      for (int c = 0; c < d.ntasks; ++c) tasks.push_back(make_uint2((uint32_t)s, (uint32_t)c));
-    }
-  }
+  const int np = (int)v.size();
+  std::vector<size_t> o_ctrl(np), o_ws(np), o_keys(np), o_out(np);
   size_t off = 0;
-  const size_t o_seg = off;
-  off += al256(sizeof(SegDesc) * nseg);
-  const size_t o_tasks = off;
-  off += al256(sizeof(uint2) * std::max<size_t>(1, tasks.size()));
-  const size_t o_del = off;
-  off += al256(4 * std::max<uint64_t>(1, del_total));
-  const size_t o_cand = off;
-  off += al256(8 * std::max<uint64_t>(1, cand_total));
-  const size_t o_ctrl = off;
-  const size_t ctrl_bytes = 4 * (8 + 2 * (size_t)nseg);
-  off += al256(ctrl_bytes);
-  const size_t hbytes = o_del;  // descriptors + tasks are staged from host
-  char* ws = nullptr;
+  for (int i = 0; i < np; ++i) {
+    o_ctrl[i] = off;
+    off += al256(v[i]->plan.ctrl_bytes);
+  }
+  const size_t ctrl_total = off;
+  for (int i = 0; i < np; ++i) {
+    o_ws[i] = off;
+    off += al256(v[i]->plan.ws_bytes);
+  }
+  for (int i = 0; i < np; ++i) {
+    o_keys[i] = off;
+    if (!v[i]->dkeys_user) off += al256(v[i]->n * 4);
+  }
+  const size_t out0 = off;
+  for (int i = 0; i < np; ++i) {
+    Req* r = v[i];
+    o_out[i] = off - out0;
+    off += al256(4) + al256(r->k * 4) + (r->user_idx ? al256(r->k * 8) : 0);
+  }
+  const size_t o_err = off - out0;  // the problems' error words, copied back with the outputs
+  off += al256(4 * (size_t)np);
+  const size_t out_total = off - out0;
+  const size_t o_desc = off;
+  const size_t desc = group_desc_bytes(np);
+  off += desc;
   size_t hcap = 0;
-  char* hst = static_cast<char*>(pinned.get(hbytes, &hcap));
-  bool ok = hst && cudaMallocAsync(reinterpret_cast<void**>(&ws), off, st) == cudaSuccess;
-  if (ok) {
-    std::memcpy(hst + o_seg, seg.data(), sizeof(SegDesc) * nseg);
-    if (!tasks.empty()) std::memcpy(hst + o_tasks, tasks.data(), sizeof(uint2) * tasks.size());
-    for (Req* r : v)
-      if (!r->dkeys_user) cudaMemcpyAsync(r->d_keys, r->hkeys, r->n * 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(ws, hst, hbytes, cudaMemcpyHostToDevice, st);
-    cudaMemsetAsync(ws + o_ctrl, 0, ctrl_bytes, st);
-    uint32_t* ctrl = reinterpret_cast<uint32_t*>(ws + o_ctrl);
-    SegArgs a;
-    std::memset(&a, 0, sizeof(a));
-    a.keys = nullptr;
-    a.seg = reinterpret_cast<const SegDesc*>(ws + o_seg);
-    a.tasks = reinterpret_cast<const uint2*>(ws + o_tasks);
-    a.n_sampler_tasks = (uint32_t)tasks.size();
-    a.nseg = (uint32_t)nseg;
-    a.del_pool = reinterpret_cast<uint32_t*>(ws + o_del);
-    a.cand_pool = reinterpret_cast<uint2*>(ws + o_cand);
-    a.ticket = ctrl;
-    a.err = ctrl + 1;
-    a.done = ctrl + 8;
-    a.seg_err = ctrl + 8 + nseg;
-    const int grid = std::min<int>(seg_grid, (int)(tasks.size() + nseg));
-    if (launch_segmented(a, std::max(1, grid), seg_smem, st) != cudaSuccess) ok = false;
-    cudaFreeAsync(ws, st);
+  char* hst = static_cast<char*>(pinned.get(out_total + desc, &hcap));
+  char* arena = nullptr;
+  const auto ta0 = std::chrono::steady_clock::now();
+  bool ok = hst && cudaMallocAsync(reinterpret_cast<void**>(&arena), off, st) == cudaSuccess;
+  if (!ok) cudaGetLastError();
+  alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta0).count();
+  if (ok && cudaMemsetAsync(arena, 0, ctrl_total, st) != cudaSuccess) ok = false;
+  std::vector<GroupItem> items(np);
+  for (int i = 0; ok && i < np; ++i) {
+    Req* r = v[i];
+    r->stream = si;
+    const void* keys = r->dkeys_user;
+    if (!keys) {
+      keys = arena + o_keys[i];
+      if (cudaMemcpyAsync(arena + o_keys[i], r->hkeys, r->n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        ok = false;
+    }
+    char* o = arena + out0 + o_out[i];
+    items[i] = {&r->plan, keys, o, o + al256(4), r->user_idx ? reinterpret_cast<int64_t*>(o + al256(4) + al256(r->k * 4))
+                                                              : nullptr,
+                arena + o_ws[i], arena + o_ctrl[i]};
   }
-  for (Req* r : v) {
-    if (r->dmem) cudaFreeAsync(r->dmem, st);
-    r->dmem = nullptr;
+  if (ok && enqueue_group(device, v[0]->plan.km, items.data(), np, hst + out_total, arena + o_desc,
+                         reinterpret_cast<uint32_t*>(arena + out0 + o_err), st) != DRTOPK_OK)
+    ok = false;
+  if (ok && cudaMemcpyAsync(hst, arena + out0, out_total, cudaMemcpyDeviceToHost, st) != cudaSuccess) ok = false;
+  if (arena) cudaFreeAsync(arena, st);
+  for (int i = 0; i < np; ++i) {
+    Req* r = v[i];
+    r->stream = si;
+    r->ev_stream = si;
+    r->hout = hst ? hst + o_out[i] : nullptr;
+    r->hout_cap = 0;  // a view into the group's staging (owned by the last request)
+    r->errp = hst ? reinterpret_cast<const uint32_t*>(hst + o_err) + i : nullptr;
+    if (!ok) r->status = DRTOPK_ECUDA;
+    cudaEventRecord(r->ev, st);
   }
-  cudaEventRecord(ev_kernels, st);
-  for (Req* r : v) {
-    if (!ok) r->status = DRTOPK_ENOMEM;
-    finish_on_copy_stream(r, ev_kernels);
-  }
-  // the descriptor staging buffer may be reused only after its copy ran:
-  // it is released with the last request of the batch (completion event
-  // recorded later on the copy stream)
+  // the staging is released with the last request (its completion event is
+  // recorded after the copy)
   if (hst) {
     v.back()->extra = hst;
     v.back()->extra_cap = hcap;
   }
+}
+
+// A grouped select whose device error word is set (DE_RETRY: its bounded
+// candidate buffers could not hold the select; any other bit) runs again
+// here, on the completion thread, with its general plan (autotuned,
+// full-size workspace on the retry handle), and its results replace the
+// staged ones.  Rare: the sample must have badly misjudged the input (heavy
+// ties around the predicted threshold, an adversarial layout).
+void drtopk_server::retry_general(Req* r) {
+  const auto t0r = std::chrono::steady_clock::now();
+  retry_general_run(r);
+  retries++;
+  retry_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0r).count();
+}
+
+void drtopk_server::retry_general_run(Req* r) {
+  r->status = DRTOPK_ECUDA;
+  if (!h_retry && drtopk_create(&h_retry, device, 0) != DRTOPK_OK) return;
+  const size_t outb = al256(4) + al256(r->k * 4) + (r->user_idx ? al256(r->k * 8) : 0);
+  char* d = nullptr;
+  const size_t kb = r->dkeys_user ? 0 : al256(r->n * 4);
+  if (cudaMalloc(&d, kb + outb) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  const void* keys = r->dkeys_user;
+  drtopk_status_t s = DRTOPK_OK;
+  if (!keys) {
+    keys = d;
+    if (cudaMemcpy(d, r->hkeys, r->n * 4, cudaMemcpyHostToDevice) != cudaSuccess) s = DRTOPK_ECUDA;
+  }
+  char* o = d + kb;
+  drtopk_params_t p;
+  drtopk_params_default(&p);
+  p.alpha = -2;
+  p.sorted = r->sorted;
+  if (s == DRTOPK_OK)
+    s = drtopk_select(h_retry, keys, r->dtype, r->n, r->k, &p, o, o + al256(4),
+                      r->user_idx ? reinterpret_cast<int64_t*>(o + al256(4) + al256(r->k * 4)) : nullptr, nullptr);
+  if (s == DRTOPK_OK) s = drtopk_sync_check(h_retry, nullptr);
+  if (s == DRTOPK_OK && cudaMemcpy(r->hout, o, outb, cudaMemcpyDeviceToHost) != cudaSuccess) s = DRTOPK_ECUDA;
+  cudaFree(d);
+  r->status = s;
+}
+
+// Memory the worker would otherwise allocate in the middle of traffic
+// (blocking its launches for milliseconds): the stream-ordered pool keeps
+// PREWARM_POOL bytes mapped (its release threshold is unlimited), and the
+// process-wide pinned cache gets two staging buffers of every size class up
+// to four times the chain output cap (a chain's staging is its outputs plus
+// its launch descriptors), once per process.
+void drtopk_server::prewarm() {
+  cudaStream_t st = streams[ST_AUX];
+  const size_t want = std::min<size_t>(PREWARM_POOL, budget ? budget / 4 : PREWARM_POOL);
+  void* p = nullptr;
+  if (cudaMallocAsync(&p, want, st) == cudaSuccess) cudaFreeAsync(p, st);
+  else cudaGetLastError();
+  cudaStreamSynchronize(st);
+  static std::once_flag once;
+  std::call_once(once, [this]() {
+    std::vector<std::pair<void*, size_t>> got;
+    for (size_t c = size_t(1) << 20; c <= 4 * GROUP_OUT_CAP; c <<= 1)
+      for (int i = 0; i < 2; ++i) {
+        size_t cap = 0;
+        void* b = pinned.get(c, &cap);
+        if (b) got.emplace_back(b, cap);
+      }
+    for (auto& g : got) pinned.put(g.first, g.second);
+  });
 }
 
 // Admission (mutex held): move requests from the queue into `out` while the
@@ -501,24 +559,34 @@ void drtopk_server::admit(std::vector<Req*>& out) {
   }
 }
 
-// Device work of the admitted requests (worker thread, unlocked): small
-// requests of this tick form one micro-batch, the others run one select each.
+// Device work of the admitted requests (worker thread, unlocked): per key
+// mode one grouped chain; a request whose plan keeps a cooperative kernel
+// runs as a select of its own.
 void drtopk_server::launch_admitted(std::vector<Req*>& v) {
-  std::vector<Req*> small;
+  std::vector<Req*> group[4];  // sampled-threshold selects by key mode
   for (Req* r : v) {
     r->ev = get_event();
+    if (r->plan.one_cta) {
+      group[r->plan.km].push_back(r);
+      continue;
+    }
     const size_t outb = al256(4) + al256(r->k * 4) + al256(r->k * 8);
     r->hout = pinned.get(outb, &r->hout_cap);
-    r->stream = r->small ? ST_BATCH : ST_SINGLE + (int)(next_single++ % NSINGLE);
+    // ordinary-launch singles round-robin over streams 1.. of the singles;
+    // a single that keeps a cooperative kernel runs in order on stream 0
+    r->stream = ST_SINGLE;
     // a select whose tail is the one-CTA kernel holds few SMs and never
     // waits on other CTAs: it runs on its own stream, beside the others
-    if (!r->small && r->plan.tail) r->stream = ST_TAIL;
+    if (r->plan.tail) r->stream = ST_TAIL;
     cudaStream_t st = streams[r->stream];
     // keys copy (host mode) and, for a request run alone, its workspace
     const size_t kb = r->dkeys_user ? 0 : al256(r->n * 4);
-    const size_t dev = kb + (r->small ? 0 : al256(r->ws_bytes));
+    const size_t dev = kb + al256(r->ws_bytes);
     r->dout = static_cast<char*>(r->hout ? outs->get(outb, &r->dout_cap) : nullptr);
-    if (!r->dout || (dev && cudaMallocAsync(reinterpret_cast<void**>(&r->dmem), dev, st) != cudaSuccess)) {
+    const auto ta0 = std::chrono::steady_clock::now();
+    const bool got = r->dout && (!dev || cudaMallocAsync(reinterpret_cast<void**>(&r->dmem), dev, st) == cudaSuccess);
+    alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta0).count();
+    if (!got) {
       cudaGetLastError();
       r->dmem = nullptr;
       r->status = DRTOPK_ENOMEM;
@@ -534,10 +602,26 @@ void drtopk_server::launch_admitted(std::vector<Req*>& v) {
     r->d_vals = reinterpret_cast<uint32_t*>(p);
     p += al256(r->k * 4);
     r->d_idx = reinterpret_cast<int64_t*>(p);
-    if (r->small) small.push_back(r);
-    else launch_single(r);
+    launch_single(r);
   }
-  if (!small.empty()) launch_batch(small, ST_BATCH);
+  for (auto& g : group) {
+    // chains of at most GROUP_OUT_CAP output bytes (staging stays in the
+    // warmed size classes)
+    std::vector<Req*> part;
+    size_t bytes = 0;
+    for (size_t i = 0; i < g.size(); ++i) {
+      Req* r = g[i];
+      const size_t ob = al256(4) + al256(r->k * 4) + (r->user_idx ? al256(r->k * 8) : 0);
+      if (!part.empty() && bytes + ob > GROUP_OUT_CAP) {
+        launch_group(part, ST_SINGLE + 1 + (int)(next_single++ % (NSINGLE - 1)));
+        part.clear();
+        bytes = 0;
+      }
+      part.push_back(r);
+      bytes += ob;
+    }
+    if (!part.empty()) launch_group(part, ST_SINGLE + 1 + (int)(next_single++ % (NSINGLE - 1)));
+  }
   // hand the requests (all with their completion events recorded) to the
   // completion thread
   {
@@ -567,7 +651,7 @@ void drtopk_server::loop() {
     }
     const auto tl0 = std::chrono::steady_clock::now();
     uint64_t ns = 0, nbr = 0;
-    for (Req* r : admitted) (r->small ? nbr : ns)++;
+    for (Req* r : admitted) (r->plan.one_cta ? nbr : ns)++;
     launch_admitted(admitted);
     admitted.clear();
     const double ms_launch = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl0).count();
@@ -623,6 +707,10 @@ void drtopk_server::complete_loop() {
       continue;
     }
     const auto tc0 = std::chrono::steady_clock::now();
+    for (size_t i = 0; i < finished.size(); ++i) {
+      Req* r = finished[i];
+      if (fq[i] == cudaSuccess && r->status == DRTOPK_OK && r->errp && *r->errp) retry_general(r);
+    }
     for (size_t i = 0; i < finished.size(); ++i) copy_out(finished[i], fq[i]);
     const double ms_complete =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc0).count();
@@ -662,8 +750,8 @@ extern "C" drtopk_status_t drtopk_server_create(drtopk_server_t* out, int device
       uint64_t thr = UINT64_MAX;
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
-    if (segmented_shape(device, &s->seg_grid, &s->seg_smem) != cudaSuccess) st = DRTOPK_ECUDA;
   }
+  if (st == DRTOPK_OK) s->prewarm();
   cudaSetDevice(cur);
   if (st != DRTOPK_OK) {
     if (s->h) drtopk_destroy(s->h);
@@ -707,6 +795,7 @@ extern "C" drtopk_status_t drtopk_server_destroy(drtopk_server_t s) {
   for (auto e : s->ev_free) cudaEventDestroy(e);
   if (s->ev_kernels) cudaEventDestroy(s->ev_kernels);
   drtopk_destroy(s->h);
+  if (s->h_retry) drtopk_destroy(s->h_retry);
   cudaSetDevice(cur);
   delete s;
   return DRTOPK_OK;
@@ -726,7 +815,6 @@ static drtopk_status_t submit_impl(drtopk_server_t s, const void* h_keys, const 
   r->user_vals = out_vals;
   r->user_idx = out_idx;
   r->dkeys_user = d_keys;
-  r->small = n <= BATCH_MAX_N && k <= (uint64_t)SEG_MAX_K;  // micro-batched through the segmented kernel
   // coarse check here (the exact workspace is sized at admission, on the
   // worker thread): the keys alone must fit the budget
   if (s->budget && (d_keys ? 0 : n * 4) + k * 12 > s->budget) {
@@ -828,5 +916,8 @@ extern "C" drtopk_status_t drtopk_server_stats(drtopk_server_t s, drtopk_server_
   // the staging cache is process-wide: report what it did since this server started
   st->pinned_allocs = s->pinned.allocs.load() - s->pin_allocs0;
   st->host_ms_pinned = (double)(s->pinned.alloc_ns.load() - s->pin_ns0) * 1e-6;
+  st->retries = s->retries;
+  st->host_ms_retry = s->retry_ms;
+  st->host_ms_alloc = s->alloc_ms;
   return DRTOPK_OK;
 }

@@ -72,7 +72,9 @@ typedef struct {
                        (cooperative grid), 2 one thread-block cluster, 3 one CTA with the sets
                        in shared memory (small problems), 4 shared GPU: as auto, but a
                        select that would take the whole GPU runs its phases in one cluster
-                       of at most 8 CTAs, so that concurrent selects overlap (served form) */
+                       of at most 8 CTAs, so that concurrent selects overlap (served form);
+                       5 ordinary launches only (sampled-threshold path): the last levels run in
+                       one CTA, so the select never waits for a share of the GPU */
 } drtopk_params_t;
 
 typedef struct {
@@ -93,7 +95,8 @@ typedef struct {
   double ms_second;
   double ms_total;
   int team_ctas;             /* CTAs that ran the phases after the sampler */
-  int team_cluster;          /* 0: the cooperative grid; 1: one thread-block cluster; 3: one CTA */
+  int team_cluster;          /* 0: the cooperative grid; 1: one thread-block cluster; 3: one CTA
+                                (shared-memory tail); 5: one ordinary CTA */
   int kernel_launches;       /* kernels the last select launched (sampler included) */
 } drtopk_stats_t;
 
@@ -278,9 +281,10 @@ DRTOPK_API drtopk_status_t drtopk_batch_describe(drtopk_batch_t b, int* h_algo, 
 
 /* ---------------------------------------------------------------------
  * Served form: continuous batching of top-k requests under an HBM budget.
- * Requests carry host keys; the server copies them into resident device
- * buffers, admits them when budget and slots allow, runs admitted requests
- * together, and returns exact results.
+ * Requests carry host keys (copied into device buffers) or device-resident
+ * keys; the server admits them when budget and slots allow, runs the
+ * requests admitted together as one chain of grouped launches (several
+ * chains overlap on the device), and returns exact results.
  * ------------------------------------------------------------------- */
 typedef struct drtopk_server* drtopk_server_t;
 
@@ -316,14 +320,17 @@ DRTOPK_API drtopk_status_t drtopk_server_usage(drtopk_server_t s, size_t* reside
 
 /* Counters of the server's worker since creation (observability). */
 typedef struct {
-  uint64_t singles;          /* requests run as one select each */
-  uint64_t batches;          /* micro-batch launches */
-  uint64_t batched;          /* requests run inside micro-batches */
+  uint64_t singles;          /* requests run as one select each (whole-GPU sorted output) */
+  uint64_t batches;          /* worker ticks that issued grouped chains */
+  uint64_t batched;          /* requests run inside grouped chains */
   uint64_t pinned_allocs;    /* pinned host buffers newly allocated (staging-cache misses) */
   uint64_t worker_ticks;     /* worker loop iterations that admitted or completed something */
   double host_ms_pinned;     /* worker time spent allocating pinned staging */
   double host_ms_launch;     /* worker time issuing device work */
   double host_ms_complete;   /* worker time copying results to the callers' buffers */
+  uint64_t retries;          /* grouped selects run again with the general plan (DE_RETRY) */
+  double host_ms_retry;      /* completion-thread time spent in those runs */
+  double host_ms_alloc;      /* worker time in stream-ordered allocations (cudaMallocAsync) */
 } drtopk_server_stats_t;
 DRTOPK_API drtopk_status_t drtopk_server_stats(drtopk_server_t s, drtopk_server_stats_t* st);
 

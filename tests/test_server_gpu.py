@@ -99,3 +99,43 @@ def test_server_budget_and_cancel():
     for i in ids:
         if i not in cancelled:
             assert res[i]["status"] == 0
+
+
+def _sampled_chunks(n, stride=64):
+    ns = (n >> 9) // stride
+    i = np.arange(ns, dtype=np.int64)
+    return i * stride + ((i * 37) & (stride - 1))
+
+
+def test_server_retries_selects_the_sample_misjudges():
+    """The served form sizes the candidate buffers of its sampled-threshold
+    selects by the sample's estimate.  Inputs that break the estimate --
+    heavy ties around the threshold (every key in one 16-bit bin), or
+    sampled chunks holding the largest keys -- make the select report that it
+    must run again, and the server reruns it with the general plan: the
+    results stay exact."""
+    import drtopksc_b200 as D
+    rng = np.random.default_rng(11)
+    n = 1 << 20
+    ties = O.gen("fewdigits", n, 5)
+    skew = rng.integers(0, 1 << 31, size=n, dtype=np.uint64).astype(np.uint32)
+    for c in _sampled_chunks(n):
+        skew[c * 512:(c + 1) * 512] = 0xFFFFFFF0 + rng.integers(0, 16, 512).astype(np.uint32)
+    nhigh = int((skew >= 0xFFFF0000).sum())
+    srv = D.Server(hbm_budget_bytes=8 << 30, max_inflight=16)
+    reqs = {}
+    for x, k, s in ((ties, 5000, False), (ties, 77, True), (skew, 3 * nhigh, False), (skew, nhigh + 1, True),
+                    (O.gen("u32", n, 6), 1000, False)):
+        reqs[srv.submit(x, k, sorted=s)] = (x, k, s)
+    srv.drain(60000)
+    got = {}
+    while True:
+        out = srv.poll()
+        if not out:
+            break
+        for res in out:
+            got[res["id"]] = res
+    srv.close()
+    assert set(got) == set(reqs)
+    for rid, (x, k, s) in reqs.items():
+        _check(got[rid], x, k, s)
