@@ -316,6 +316,100 @@ def bench_served(D, torch, dev, stream, args):
     return out
 
 
+def bench_extras(D, torch, dev, stream, h, peak, log2n):
+    """The other configurations BASELINE names, reported beside the headline
+    (each: ms per call, keys/s, fraction of the measured HBM roofline over
+    the algorithmic bytes 4N + output):
+      C1   N=2^20 uint32 uniform, k=128: latency of one call, and the share of
+           the phases after the sampler;
+      C2b  N=2^30 normal(2^31, 2^28) uint32, k=2^0..2^24;
+      C3   N=2^28 float32 uniform [0,1) and normal(0,1), and few-digits uint32
+           (top 24 bits fixed), k in {16, 256, 4096, 65536}: radix (autotuned),
+           bucket and bitonic (k <= 2048), sorted values with indices;
+      sorted_idx  N=2^30 uint32 uniform, sorted top-k with int64 indices,
+           k=2^0..2^24 (output bytes 12k counted)."""
+    sp = stream.cuda_stream or None
+    g = torch.Generator(device=dev)
+
+    def timed(keys, dt, n, k, p, want_idx, reps):
+        kth = torch.empty(1, dtype=torch.int32, device=dev)
+        vals = torch.empty(k, dtype=torch.int32, device=dev)
+        idx = torch.empty(k, dtype=torch.int64, device=dev) if want_idx else None
+        ip = idx.data_ptr() if want_idx else None
+        for _ in range(2):
+            h.select_raw(keys.data_ptr(), dt, n, k, p, kth.data_ptr(), vals.data_ptr(), ip, sp)
+        a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            h.select_raw(keys.data_ptr(), dt, n, k, p, kth.data_ptr(), vals.data_ptr(), ip, sp)
+        b2.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = a.elapsed_time(b2) / reps
+        st = h.stats()
+        outb = 4 * k + (8 * k if want_idx else 0)
+        return {"ms": round(ms, 4), "keys_per_s": n / (ms * 1e-3),
+                "frac_of_measured_hbm": round((4.0 * n + outb) / (ms * 1e-3) / (peak * 1e9), 4),
+                "algo": st["algo"], "alpha": st["alpha"], "beta": st["beta"], "candidates": st["n_candidates"],
+                "ms_sample": round(st["ms_sample"], 4), "ms_after_sampler": round(st["ms_total"] - st["ms_sample"], 4)}
+
+    out = {}
+    # C1
+    g.manual_seed(1)
+    n1 = 1 << 20
+    k1 = torch.randint(-(1 << 31), 1 << 31, (n1,), dtype=torch.int32, device=dev, generator=g)
+    r = timed(k1, D.U32, n1, 128, D.autotune(n1, 128, D.U32, D.params(alpha=-2)), False, 200)
+    r["after_sampler_share"] = round(r["ms_after_sampler"] / max(1e-9, r["ms_sample"] + r["ms_after_sampler"]), 3)
+    out["C1_n2^20_k128"] = r
+    del k1
+    # C2b
+    if log2n == 30:
+        g.manual_seed(2)
+        n2 = 1 << 30
+        z = torch.empty(n2, dtype=torch.int32, device=dev)
+        for c in range(0, n2, 1 << 27):  # in slices: the float64 draw of 2^30 normals needs 8 GB
+            zz = torch.randn(1 << 27, dtype=torch.float64, device=dev, generator=g)
+            z[c:c + (1 << 27)] = (zz * 2.0 ** 28 + 2.0 ** 31).round().clamp(0, 2 ** 32 - 1).to(torch.int64).to(torch.int32)
+        del zz
+        rows = {}
+        tot_ms = 0.0
+        for i in range(25):
+            k = 1 << i
+            rr = timed(z, D.U32, n2, k, D.autotune(n2, k, D.U32, D.params(alpha=-2)), False, 3)
+            rows[str(k)] = rr
+            tot_ms += rr["ms"]
+        out["C2b_normal_n2^30"] = {"keys_per_s_sweep": 25 * n2 / (tot_ms * 1e-3), "per_k": rows}
+        del z
+    # C3
+    n3 = 1 << 28
+    c3 = {}
+    for dist in ("f32u", "f32n", "fewdigits"):
+        g.manual_seed(3)
+        if dist == "f32u":
+            x = torch.rand(n3, dtype=torch.float32, device=dev, generator=g)
+            dt = D.F32
+        elif dist == "f32n":
+            x = torch.randn(n3, dtype=torch.float32, device=dev, generator=g)
+            dt = D.F32
+        else:
+            x = (torch.randint(0, 256, (n3,), dtype=torch.int32, device=dev, generator=g) | (0xABCDEF << 8)).to(
+                torch.int32)
+            dt = D.U32
+        for k in (16, 256, 4096, 65536):
+            for algo in ("radix", "radix-ref", "bucket", "bitonic"):
+                if algo == "bitonic" and k > 2048:
+                    continue
+                if algo == "radix":  # autotuned
+                    p = D.autotune(n3, k, dt, D.params(alpha=-2, sorted=True))
+                elif algo == "radix-ref":  # the reference's own parameters (main.cu:83-89)
+                    p = D.params(sorted=True)
+                else:
+                    p = D.params(algo=algo, sorted=True)
+                c3[f"{dist}/k{k}/{algo}"] = timed(x, dt, n3, k, p, True, 5)
+        del x
+    out["C3_n2^28_sorted_idx"] = c3
+    return out
+
+
 METRIC = "keys/s (exact top-k over N=2^30 uint32 uniform keys, k sweep 2^0..2^24)"
 
 
@@ -444,6 +538,7 @@ def main():
     ap.add_argument("--no-table", action="store_true", help="skip the per-k tables after the timed region")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-form measurement")
+    ap.add_argument("--no-extras", action="store_true", help="skip the other BASELINE configurations")
     ap.add_argument("--batch-segments", type=int, default=4096)
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-pool", type=int, default=48)
@@ -578,6 +673,29 @@ def main():
     # kernels one step launches (the same plans as the timed sweep)
     launches_per_step = sum(sweep[str(k)]["launches"] for k in ks) if sweep else None
 
+    # sorted top-k with int64 indices over the same keys (12 output bytes per k)
+    sorted_idx = {}
+    if not args.no_extras and rank == 0 and world == 1:
+        idx = torch.empty(kmax, dtype=torch.int64, device=dev)
+        tot_ms = 0.0
+        for i, k in enumerate(ks):
+            pk = D.autotune(n, k, D.U32, D.params(alpha=-2, sorted=True))
+            for _ in range(2):
+                h.select_raw(keys.data_ptr(), D.U32, n, k, pk, kth.data_ptr(), vals.data_ptr(), idx.data_ptr(), sp)
+            a, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(3):
+                h.select_raw(keys.data_ptr(), D.U32, n, k, pk, kth.data_ptr(), vals.data_ptr(), idx.data_ptr(), sp)
+            b2.record(stream)
+            torch.cuda.synchronize(dev)
+            kms = a.elapsed_time(b2) / 3
+            tot_ms += kms
+            sorted_idx[str(k)] = {"ms": round(kms, 4), "frac_of_measured_hbm":
+                                  round((4.0 * n + 12.0 * k) / (kms * 1e-3) / (peak * 1e9), 4)}
+        h.sync_check(stream)
+        sorted_idx = {"keys_per_s_sweep": len(ks) * n / (tot_ms * 1e-3), "per_k": sorted_idx}
+        del idx
+
     # ---------------- end to end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -619,10 +737,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline()
 
-    batched = served = None
+    batched = served = extras = None
     if rank == 0 and world == 1:
         del keys
         torch.cuda.empty_cache()
+        if not args.no_extras:
+            extras = bench_extras(D, torch, dev, stream, h, peak, args.log2n)
+            torch.cuda.empty_cache()
         if not args.no_batch:
             batched = bench_batched(D, torch, dev, stream, args)
             torch.cuda.empty_cache()
@@ -655,6 +776,8 @@ def main():
             "gpu_launches": launches_per_step * args.steps if launches_per_step else None,
             "k_sweep": sweep,
             "k_sweep_reference_alpha": sweep_ref,
+            "sorted_with_indices": sorted_idx,
+            "extra_configs": extras,
             "batched": batched,
             "served": served,
         }

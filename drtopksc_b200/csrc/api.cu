@@ -1409,7 +1409,12 @@ extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_
     const double ks = dk / 64.0;
     const double cand = dk + 64.0 * (6.0 * std::sqrt(ks) + 16.0) + dn / 65536.0;
     const double c = 4.0 * dn / 1.1 + 50.0 * TAIL_BYTES_PER_US + 73.0 * cand;
-    if (c < best) { best = c; best_emit = true; }
+    // float keys crowd into few exponent bins: the delegate paths' fixed
+    // threshold digits can then admit a large share of the keys (uniform
+    // [0,1) keys: ~1/512 per 16-bit bin), while the sampled threshold adapts
+    // to the data and its tight level 0 spreads the candidates; from 2^22
+    // float keys the sampled-threshold path is taken whatever the model says
+    if (c < best || (dtype == DRTOPK_F32 && n >= (1ull << 22))) { best = c; best_emit = true; }
   }
   if (best_emit) {
     p->path = 4;
