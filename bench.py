@@ -762,7 +762,8 @@ def main():
                 {"auto": "autotuner (drtopk_autotune)", "ref": "reference formula (main.cu:83)",
                  "emit": "sampled-threshold path (path 4) for every k"}[args.alpha_mode]),
             "outputs": "the k-th value and the k largest values (unsorted), per call",
-            "roofline": {"bound": "hbm", "kernel": "k_sample (delegate sampler)", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "the streaming pass: k_sample (delegate sampler; sample passes + "
+                                                    "k_emit on the sampled-threshold path)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic_bytes, "algorithmic_bytes_per_launch": 4 * n,
                          "ms_per_launch": sample_ms_per_launch,

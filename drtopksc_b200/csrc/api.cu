@@ -902,7 +902,8 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
   fill_args(P, d_keys, d_kth, d_vals, d_idx, ws, ctrl, &a);
   // ---- sampled-threshold path: sample, predict, emit, then the second select
   if (P.path == PATH_EMIT) {
-    if (ev) cudaEventRecord(ev[1], st);
+    // the streaming interval (ev[0] -> ev[1]) is the two sample passes and
+    // the appending pass, the counterpart of the delegate paths' sampler
     void* args[] = {&a};
     drtopk_status_t s = DRTOPK_OK;
     if (cudaLaunchKernel(split_ptr(P.km, SK_PRESAMPLE), dim3(P.presample_grid), dim3(FUSED_THREADS), args, 0, st) !=
@@ -910,7 +911,10 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
         cudaLaunchKernel(split_ptr(P.km, SK_PRESAMPLE2), dim3(P.presample_grid), dim3(FUSED_THREADS), args, 0, st) !=
             cudaSuccess ||
         cudaLaunchKernel(split_ptr(P.km, SK_EMIT), dim3(P.emit_grid), dim3(FUSED_THREADS), args,
-                         split_smem(P.nb, SK_EMIT), st) != cudaSuccess ||
+                         split_smem(P.nb, SK_EMIT), st) != cudaSuccess)
+      s = DRTOPK_ECUDA;
+    if (ev) cudaEventRecord(ev[1], st);
+    if (s == DRTOPK_OK &&
         cudaLaunchKernel(split_ptr(P.km, SK_CAND_HIST), dim3(P.hist_grid), dim3(FUSED_THREADS), args,
                          split_smem(P.nb, SK_CAND_HIST), st) != cudaSuccess)
       s = DRTOPK_ECUDA;

@@ -79,6 +79,8 @@ def test_autotune_choices_are_valid():
         m = (n + s - 1) // s
         if p.path == 1:
             assert m >= k
+        elif p.path == 4:  # sampled threshold: large k only, no delegate vector
+            assert k >= 1 << 16
         else:
             assert p.path == 2 and p.alpha <= 16 and 2 * m >= 1
 
