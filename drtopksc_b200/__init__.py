@@ -55,7 +55,8 @@ class Stats(ctypes.Structure):
                 ("levels_first", ctypes.c_int), ("levels_second", ctypes.c_int), ("device_error", ctypes.c_uint32),
                 ("ms_sample", ctypes.c_double), ("ms_first", ctypes.c_double), ("ms_concat", ctypes.c_double),
                 ("ms_second", ctypes.c_double), ("ms_total", ctypes.c_double), ("team_ctas", ctypes.c_int),
-                ("team_cluster", ctypes.c_int), ("kernel_launches", ctypes.c_int)]
+                ("team_cluster", ctypes.c_int), ("kernel_launches", ctypes.c_int),
+                ("sample_stride", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -189,7 +189,7 @@ static bool tail_ready(int device, int km) {
 
 // the ordinary (non-cooperative) kernels of split mode
 enum SplitKernel : int {
-  SK_GATHER = 0, SK_FILTER = 1, SK_LEVEL_HIST = 2, SK_SPLIT0 = 3, SK_EMIT = 4, SK_PRESAMPLE = 5, SK_PRESAMPLE2 = 6,
+  SK_GATHER = 0, SK_FILTER = 1, SK_LEVEL_HIST = 2, SK_SPLIT0 = 3, SK_EMIT = 4, SK_PRESAMPLE = 5, SK_PREREFINE = 6,
   SK_CAND_HIST = 7
 };
 static void* split_ptr(int km, int which) {
@@ -200,7 +200,7 @@ static void* split_ptr(int km, int which) {
     case SK_SPLIT0: return const_cast<void*>(ks.split0);
     case SK_EMIT: return const_cast<void*>(ks.emit);
     case SK_PRESAMPLE: return const_cast<void*>(ks.presample);
-    case SK_PRESAMPLE2: return const_cast<void*>(ks.presample2);
+    case SK_PREREFINE: return const_cast<void*>(ks.prerefine);
     case SK_CAND_HIST: return const_cast<void*>(ks.cand_hist);
     default: return const_cast<void*>(ks.gather);
   }
@@ -208,7 +208,7 @@ static void* split_ptr(int km, int which) {
 
 // dynamic shared memory of a split-mode kernel: histogram words + warp stages
 static size_t split_smem(int nb, int which) {
-  if (which == SK_PRESAMPLE || which == SK_PRESAMPLE2) return 0;
+  if (which == SK_PRESAMPLE || which == SK_PREREFINE) return 0;
   const size_t h = (size_t)std::max(nb, 256) * 4;
   if (which == SK_FILTER) return h + SPLIT_FILTER_SMEM;
   if (which == SK_GATHER) return h + SPLIT_GATHER_SMEM;
@@ -337,9 +337,14 @@ drtopk_status_t make_plan(uint64_t n, uint64_t k, drtopk_dtype_t dtype, const dr
     // sampled-threshold concatenation: no delegate vector (alpha unused)
     P->path = PATH_EMIT;
     P->alpha = 0;
-    // sampled keys: one 512-key chunk in PRE_STRIDE; the predicted threshold
-    // must keep k scaled to the sample plus a six-sigma margin above it
-    const uint64_t ns_keys = ((n >> 9) / PRE_STRIDE) * 512;
+    // sampled keys: one 512-key chunk in pre_stride, the sparsest stride in
+    // [PRE_STRIDE_MIN, PRE_STRIDE_MAX] that keeps PRE_SAMPLE_CHUNKS chunks
+    // (the sample passes' cost falls with the stride; the six-sigma margin
+    // and the candidates it admits grow only with its square root); the
+    // predicted threshold must keep k scaled to the sample plus a six-sigma
+    // margin above it
+    P->pre_stride = pre_stride_for(n);
+    const uint64_t ns_keys = ((n >> 9) / P->pre_stride) * 512;
     const double ks = ns_keys ? (double)k * (double)ns_keys / (double)n : 0.0;
     const double t = std::ceil(ks + 6.0 * std::sqrt(ks) + 16.0);
     P->pre_target = (uint32_t)std::min(t, 4294967295.0);
@@ -408,7 +413,8 @@ void layout(Plan* P, bool want_idx) {
   P->run_words = 3 * P->hist_words + (MAX_LEVELS + 2) + 1 + 4;
   size_t ctrl_words = CTRL_HDR_WORDS + 4 * (size_t)P->run_words + 8 * 256;
   P->pre_hist_word = ctrl_words;
-  ctrl_words += 512;  // sampled-threshold path: two 256-bin histograms of the key sample
+  ctrl_words += PRE_STATE + PRE_STATE_WORDS;  // sampled-threshold path: one 256-bin histogram per byte level
+                                               // of the key sample, then the walk's state
   P->off_ctrl = take(ctrl_words * 4);
   P->ctrl_bytes = ctrl_words * 4;
   uint64_t ncand_cap = 0;
@@ -586,7 +592,7 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
         split_grid(di, P->km, SK_CAND_HIST, split_smem(P->nb, SK_CAND_HIST), &P->hist_grid) != cudaSuccess)
       return DRTOPK_ECUDA;
     // persistent grid over the sampled chunks, PRE_ROUND per warp and round
-    const uint64_t nsw = ((n >> 9) / PRE_STRIDE + PRE_ROUND * SPLIT_WARPS - 1) / (PRE_ROUND * SPLIT_WARPS);
+    const uint64_t nsw = ((n >> 9) / P->pre_stride + PRE_ROUND * SPLIT_WARPS - 1) / (PRE_ROUND * SPLIT_WARPS);
     P->presample_grid =
         (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)di->sms * PRE_CTAS_PER_SM, nsw));
     const uint64_t nct = ((n + 511) / 512 + SPLIT_WARPS - 1) / SPLIT_WARPS;
@@ -851,6 +857,7 @@ static void fill_args(const Plan& P, const void* d_keys, void* d_kth, void* d_va
   a.tail_flag = cw + CW_TAIL;
   a.pre_hist = cw + P.pre_hist_word;
   a.pre_target = P.pre_target;
+  a.pre_stride = P.pre_stride ? P.pre_stride : PRE_STRIDE_MIN;
   a.bounded = P.bounded;
   a.phase_lo = 1;
   a.phase_hi = 3;
@@ -902,16 +909,21 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
   fill_args(P, d_keys, d_kth, d_vals, d_idx, ws, ctrl, &a);
   // ---- sampled-threshold path: sample, predict, emit, then the second select
   if (P.path == PATH_EMIT) {
-    // the streaming interval (ev[0] -> ev[1]) is the two sample passes and
-    // the appending pass, the counterpart of the delegate paths' sampler
+    // the streaming interval (ev[0] -> ev[1]) is the sample passes and the
+    // appending pass, the counterpart of the delegate paths' sampler
     void* args[] = {&a};
     drtopk_status_t s = DRTOPK_OK;
     if (cudaLaunchKernel(split_ptr(P.km, SK_PRESAMPLE), dim3(P.presample_grid), dim3(FUSED_THREADS), args, 0, st) !=
-            cudaSuccess ||
-        cudaLaunchKernel(split_ptr(P.km, SK_PRESAMPLE2), dim3(P.presample_grid), dim3(FUSED_THREADS), args, 0, st) !=
-            cudaSuccess ||
-        cudaLaunchKernel(split_ptr(P.km, SK_EMIT), dim3(P.emit_grid), dim3(FUSED_THREADS), args,
-                         split_smem(P.nb, SK_EMIT), st) != cudaSuccess)
+        cudaSuccess)
+      s = DRTOPK_ECUDA;
+    for (int level = 1; level < PRE_LEVELS && s == DRTOPK_OK; ++level) {
+      void* rargs[] = {&a, &level};
+      if (cudaLaunchKernel(split_ptr(P.km, SK_PREREFINE), dim3(P.presample_grid), dim3(FUSED_THREADS), rargs, 0,
+                           st) != cudaSuccess)
+        s = DRTOPK_ECUDA;
+    }
+    if (s == DRTOPK_OK && cudaLaunchKernel(split_ptr(P.km, SK_EMIT), dim3(P.emit_grid), dim3(FUSED_THREADS), args,
+                                           split_smem(P.nb, SK_EMIT), st) != cudaSuccess)
       s = DRTOPK_ECUDA;
     if (ev) cudaEventRecord(ev[1], st);
     if (s == DRTOPK_OK &&
@@ -1027,7 +1039,9 @@ drtopk_status_t enqueue_select(const Plan& P, int device, const void* d_keys, vo
 
 // ------------------------------------------------------------ grouped selects
 // Stages of a grouped sampled-threshold chain, in launch order.
-enum GroupStage : int { GS_PRESAMPLE = 0, GS_PRESAMPLE2, GS_EMIT, GS_CAND_HIST, GS_SPLIT0, GS_LAST, GS_COUNT };
+enum GroupStage : int {
+  GS_PRESAMPLE = 0, GS_REFINE1, GS_REFINE2, GS_REFINE3, GS_EMIT, GS_CAND_HIST, GS_SPLIT0, GS_LAST, GS_COUNT
+};
 
 size_t group_desc_bytes(int nprob) {
   return align256(sizeof(FusedArgs) * (size_t)nprob) + align256(4 * (size_t)GS_COUNT * (nprob + 1));
@@ -1042,8 +1056,10 @@ static uint32_t group_ctas(const Plan& P, int stage) {
   auto clampc = [](uint64_t v, uint64_t cap) { return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(v, cap)); };
   switch (stage) {
     case GS_PRESAMPLE:
-    case GS_PRESAMPLE2: {
-      const uint64_t ns = (n >> 9) / PRE_STRIDE;
+    case GS_REFINE1:
+    case GS_REFINE2:
+    case GS_REFINE3: {
+      const uint64_t ns = (n >> 9) / P.pre_stride;
       return clampc((ns + PRE_ROUND * SPLIT_WARPS - 1) / (PRE_ROUND * SPLIT_WARPS), (uint64_t)P.presample_grid);
     }
     case GS_EMIT:  // at least eight 512-key chunks per warp
@@ -1085,10 +1101,10 @@ drtopk_status_t enqueue_group(int device, int km, const GroupItem* items, int np
   if (cudaMemcpyAsync(d_desc, h_stage, group_desc_bytes(nprob), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return DRTOPK_ECUDA;
   const KernelSet& ks = kernels(km);
-  const void* fns[GS_COUNT] = {ks.presample_g, ks.presample2_g, ks.emit_g, ks.cand_hist_g, ks.split0_g,
-                               ks.fused_one_g};
+  const void* fns[GS_COUNT] = {ks.presample_g, ks.prerefine_g,  ks.prerefine_g, ks.prerefine_g,
+                               ks.emit_g,      ks.cand_hist_g, ks.split0_g,    ks.fused_one_g};
   const int nb = items[0].P->nb;
-  const size_t smem[GS_COUNT] = {0, 0, split_smem(nb, SK_EMIT), split_smem(nb, SK_CAND_HIST),
+  const size_t smem[GS_COUNT] = {0, 0, 0, 0, split_smem(nb, SK_EMIT), split_smem(nb, SK_CAND_HIST),
                                  split_smem(nb, SK_SPLIT0), smem_last};
   if (!fused_one_group_ready(device, km, smem_last)) return DRTOPK_ECUDA;
   const uint32_t* dpre = reinterpret_cast<const uint32_t*>(d_desc + align256(sizeof(FusedArgs) * (size_t)nprob));
@@ -1097,7 +1113,8 @@ drtopk_status_t enqueue_group(int device, int km, const GroupItem* items, int np
     g.probs = reinterpret_cast<const FusedArgs*>(d_desc);
     g.prefix = dpre + s * (nprob + 1);
     g.nprob = (uint32_t)nprob;
-    void* args[] = {&g};
+    int level = s - GS_PRESAMPLE;  // byte level of the refine stages (k_prerefine_g's second argument)
+    void* args[] = {&g, &level};
     if (cudaLaunchKernel(fns[s], dim3(tot[s]), dim3(FUSED_THREADS), args, smem[s], st) != cudaSuccess)
       return DRTOPK_ECUDA;
   }
@@ -1196,7 +1213,8 @@ extern "C" drtopk_status_t drtopk_sync_check(drtopk_handle_t h, void* stream) {
 
 // kernels one select of plan P launches (enqueue_select's launch sequence)
 static int plan_launches(const Plan& P) {
-  if (P.path == PATH_EMIT) return 6;  // k_presample, k_presample2, k_emit, k_cand_hist, k_split0, k_fused
+  // k_presample, k_prerefine x 3, k_emit, k_cand_hist, k_split0, k_fused
+  if (P.path == PATH_EMIT) return 5 + PRE_LEVELS;
   const bool sampler = P.path != PATH_PLAIN && !(P.path == PATH_BITONIC && P.normal);
   int n = sampler ? 1 : 0;
   if (P.path == PATH_BITONIC || P.tail || P.cluster > 0 || !P.split) return n + 1;
@@ -1244,6 +1262,7 @@ extern "C" drtopk_status_t drtopk_last_stats(drtopk_handle_t h, drtopk_stats_t* 
     st->team_ctas = P.tail ? TAIL_CLUSTER : (P.cluster > 0 ? P.cluster : (P.one_cta ? 1 : P.fused_grid));
     st->team_cluster = P.tail ? 3 : (P.cluster > 0 ? 1 : (P.one_cta ? 5 : 0));
     st->kernel_launches = plan_launches(P);
+    st->sample_stride = P.path == PATH_EMIT ? (int)P.pre_stride : 0;
   }
   cudaSetDevice(cur);
   return s;

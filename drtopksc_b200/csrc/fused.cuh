@@ -71,8 +71,9 @@ struct FusedArgs {
   int first_pre;          // split mode: the first select runs in k_level_hist / k_filter
   int split0;             // split mode: level 0 of the second select runs in k_split0
   int direct0;            // ... writing its top entries straight to the (unsorted) output
-  uint32_t* pre_hist;     // [2][256] sampled-threshold path: top / second byte counts of the key sample
+  uint32_t* pre_hist;     // [4][256] sampled-threshold path: byte-level counts of the key sample
   uint32_t pre_target;    // sampled keys that must lie at or above the predicted threshold
+  uint32_t pre_stride;    // one 512-key chunk in pre_stride is sampled (a power of two)
   int bounded;            // candidate buffers sized by the sample's estimate: no device fallback
   GridBar gb;
 };
@@ -1057,24 +1058,88 @@ __global__ void __launch_bounds__(FUSED_THREADS, 4) k_gather(FusedArgs a) {
 // of subranges where only Max does -- is exactly the set of keys >= t, so
 // the pass appends every key >= t_pred together with its index:
 //   k_presample   top-byte histogram of a strided sample of the keys (one
-//                 512-key chunk in PRE_STRIDE, at a rotating offset);
-//   k_presample2  the byte picked from it, then the second-byte histogram
-//                 of the sampled keys inside it (the sample is L2-resident);
-//   k_emit        t_pred = the 16-bit prefix boundary at which the sample
-//                 holds pre_target keys (k scaled to the sample plus a
-//                 six-sigma margin, set by the host), then one streaming
-//                 pass appending every key >= t_pred, with the level-0
+//                 512-key chunk in pre_stride, at a rotating offset);
+//   k_prerefine   (levels 1..3) the bytes picked so far, then the next
+//                 byte's histogram of the sampled keys under that prefix
+//                 (the sample is L2-resident).  Levels 2 and 3 run only
+//                 while the picked bin still holds more than
+//                 PRE_REFINE_KEYS keys' worth of the sample -- inputs whose
+//                 keys share their top bytes (few distinct values, narrow
+//                 ranges) -- and return at once otherwise;
+//   k_emit        t_pred = the prefix boundary at which the sample holds
+//                 pre_target keys (k scaled to the sample plus a six-sigma
+//                 margin, set by the host), then one streaming pass
+//                 appending every key >= t_pred, with the level-0
 //                 histogram of the second select, as the gather does.
+// The last CTA to finish a sample pass makes the level's pick for all
+// later kernels (pre_state): the next refine level's CTAs read one word to
+// learn whether they have work, and k_emit reads the finished threshold.
 // k_split0 and the last levels of k_fused then run as in split mode.  The
 // count of appended keys proves the prediction: at least k of them means
 // t_pred <= the k-th key, so every key of the top k is a candidate.  With
 // fewer, k_split0 does nothing and k_fused selects over all keys (plain
 // radix select), so the result is exact whatever the input.
-constexpr int PRE_STRIDE = 64;
+constexpr uint32_t PRE_STRIDE_MIN = 64;    // the sample is at most 1/64 of the keys
+constexpr uint32_t PRE_STRIDE_MAX = 512;   // and at least 1/512
+constexpr uint64_t PRE_SAMPLE_CHUNKS = 4096;
 constexpr int PRE_ROUND = 4;     // sampled chunks in flight per warp
 constexpr int PRE_CTAS_PER_SM = 2;
+constexpr int PRE_LEVELS = 4;    // byte levels of the predicted threshold (at least 2 are used)
+// a picked bin holding more keys than this (estimated from the sample) is
+// refined by one more sample pass: one pass over the L2-resident sample
+// costs about what appending this many extra candidates does
+constexpr uint64_t PRE_REFINE_KEYS = 1ull << 20;
+// control words after the PRE_LEVELS histograms (pre_hist + PRE_STATE):
+// [0, PRE_LEVELS) CTAs done per level, then the walk's state
+constexpr int PRE_STATE = 256 * PRE_LEVELS;
+constexpr int PS_DONE = PRE_LEVELS;  // bytes of the finished threshold (0: not finished)
+constexpr int PS_PREFIX = PRE_LEVELS + 1;  // picked bytes so far (the threshold once finished)
+constexpr int PRE_STATE_WORDS = PRE_LEVELS + 2;
 
-DRTOPK_DEV uint64_t pre_chunk(uint64_t i) { return i * PRE_STRIDE + ((i * 37u) & (PRE_STRIDE - 1)); }
+// sampling stride for n keys: the sparsest power of two in [PRE_STRIDE_MIN,
+// PRE_STRIDE_MAX] that still samples PRE_SAMPLE_CHUNKS chunks
+inline uint32_t pre_stride_for(uint64_t n) {
+  uint32_t s = PRE_STRIDE_MIN;
+  while (s < PRE_STRIDE_MAX && (n >> 9) / (2ull * s) >= PRE_SAMPLE_CHUNKS) s <<= 1;
+  return s;
+}
+
+DRTOPK_DEV uint64_t pre_chunk(uint64_t i, uint32_t stride) {
+  return i * stride + ((i * 37u) & (stride - 1));
+}
+
+// After the pass of byte level `level` (by `ncta` CTAs of this select): the
+// last CTA to finish walks levels 0..level over the complete histograms and
+// publishes the prefix (and, when the walk ends here, the threshold's byte
+// count).  Level l picks the bin holding the remaining target rank; from
+// level 1 on the walk ends once the picked bin is small enough, or at the
+// last level.  Block-collective.
+DRTOPK_DEV void pre_publish(const FusedArgs& a, int level, uint32_t ncta) {
+  __shared__ uint32_t s_last;
+  uint32_t* st = a.pre_hist + PRE_STATE;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&st[level], 1u) == ncta - 1 ? 1u : 0u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  uint32_t prefix = 0, r = a.pre_target;
+  int done = 0;
+  for (int l = 0; l <= level; ++l) {
+    const Pick p = block_pick<false>(a.pre_hist + 256 * l, 256, r);
+    prefix = (prefix << 8) | p.b;
+    r = r > p.above ? r - p.above : 1u;
+    if (l >= 1 && (l == PRE_LEVELS - 1 || (uint64_t)p.cnt * a.pre_stride <= PRE_REFINE_KEYS)) {
+      done = l + 1;
+      break;
+    }
+  }
+  if (threadIdx.x == 0) {
+    st[PS_PREFIX] = prefix;
+    __threadfence();
+    if (done) st[PS_DONE] = (uint32_t)done;
+  }
+}
 
 // 16 keys of 512-key chunk `ch` held by this lane (load q: keys
 // ch*512 + 128 q + 4 lane + e), mapped to keys; positions >= n read as key 0
@@ -1097,13 +1162,15 @@ DRTOPK_DEV void chunk_keys(const FusedArgs& a, uint64_t ch, uint64_t pol, uint32
 }
 
 template <int KM>
-DRTOPK_DEV void presample_pass(const FusedArgs& a, int level, uint32_t b0, uint32_t (*s_h)[256], uint32_t cta,
+// Histogram of byte `level` of the sampled keys whose higher bytes equal
+// `prefix` (all keys at level 0), added to pre_hist row `level`.
+DRTOPK_DEV void presample_pass(const FusedArgs& a, int level, uint32_t prefix, uint32_t (*s_h)[256], uint32_t cta,
                                uint32_t ncta) {
   const unsigned lane = lane_id();
   const int wib = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < SPLIT_WARPS * 256; i += blockDim.x) (&s_h[0][0])[i] = 0;
   __syncthreads();
-  const uint64_t ns = (a.n >> 9) / PRE_STRIDE;
+  const uint64_t ns = (a.n >> 9) / a.pre_stride;
   const uint64_t gw = (uint64_t)cta * SPLIT_WARPS + wib, nw = (uint64_t)ncta * SPLIT_WARPS;
   // PRE_ROUND sampled chunks per warp and round, all loaded before any is
   // counted (the pass is latency-bound); a small persistent grid keeps the
@@ -1113,7 +1180,7 @@ DRTOPK_DEV void presample_pass(const FusedArgs& a, int level, uint32_t b0, uint3
 #pragma unroll
     for (int c = 0; c < PRE_ROUND; ++c) {
       const uint64_t ic = i + (uint64_t)c * nw;
-      const uint64_t cb = pre_chunk(ic < ns ? ic : i) << 9;
+      const uint64_t cb = pre_chunk(ic < ns ? ic : i, a.pre_stride) << 9;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const uint64_t base = cb + 128 * q + 4 * lane;
@@ -1126,6 +1193,7 @@ DRTOPK_DEV void presample_pass(const FusedArgs& a, int level, uint32_t b0, uint3
         }
       }
     }
+    const int sh = 24 - 8 * level;  // the byte counted; the prefix is every bit above it
 #pragma unroll
     for (int c = 0; c < PRE_ROUND; ++c) {
       if (i + (uint64_t)c * nw >= ns) break;  // warp-uniform
@@ -1134,8 +1202,25 @@ DRTOPK_DEV void presample_pass(const FusedArgs& a, int level, uint32_t b0, uint3
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const uint32_t key = to_key<KM>(k[c][q][e]);
-          if (level == 0) hist_add_warp(s_h[wib], key >> 24);
-          else if ((key >> 24) == b0) atomicAdd(&s_h[wib][(key >> 16) & 255u], 1u);
+          if (level == 0) {
+            hist_add_warp(s_h[wib], key >> 24);
+          } else {
+            // the whole warp takes part: one vote when every matching lane
+            // counts the same byte (keys crowding into a few values), else
+            // one shared atomic per matching lane (sparse matches)
+            const bool hit = (key >> (sh + 8)) == prefix;
+            const uint32_t bin = (key >> sh) & 255u;
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (m) {
+              const int lead = __ffs(m) - 1;
+              const uint32_t b0 = __shfl_sync(0xffffffffu, bin, lead);
+              if (__all_sync(0xffffffffu, !hit || bin == b0)) {
+                if ((int)lane == lead) atomicAdd(&s_h[wib][b0], (uint32_t)__popc(m));
+              } else if (hit) {
+                atomicAdd(&s_h[wib][bin], 1u);
+              }
+            }
+          }
         }
     }
   }
@@ -1153,13 +1238,16 @@ DRTOPK_DEV void presample_body(const FusedArgs& a, uint32_t cta, uint32_t ncta) 
   __shared__ uint32_t s_h[SPLIT_WARPS][256];
   if (cta == 0 && threadIdx.x == 0) stamp(a.stats, 16);
   presample_pass<KM>(a, 0, 0u, s_h, cta, ncta);
+  pre_publish(a, 0, ncta);
 }
 
 template <int KM>
-DRTOPK_DEV void presample2_body(const FusedArgs& a, uint32_t cta, uint32_t ncta) {
+DRTOPK_DEV void prerefine_body(const FusedArgs& a, int level, uint32_t cta, uint32_t ncta) {
   __shared__ uint32_t s_h2[SPLIT_WARPS][256];
-  const Pick p0 = block_pick<false>(a.pre_hist, 256, a.pre_target);
-  presample_pass<KM>(a, 1, (uint32_t)p0.b, s_h2, cta, ncta);
+  const uint32_t* st = a.pre_hist + PRE_STATE;
+  if (ld_cg_u32(st + PS_DONE)) return;  // the threshold needs no further byte
+  presample_pass<KM>(a, level, ld_cg_u32(st + PS_PREFIX), s_h2, cta, ncta);
+  pre_publish(a, level, ncta);
 }
 
 template <int KM>
@@ -1168,8 +1256,8 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_presample(FusedArgs a) {
 }
 
 template <int KM>
-__global__ void __launch_bounds__(FUSED_THREADS) k_presample2(FusedArgs a) {
-  presample2_body<KM>(a, blockIdx.x, gridDim.x);
+__global__ void __launch_bounds__(FUSED_THREADS) k_prerefine(FusedArgs a, int level) {
+  prerefine_body<KM>(a, level, blockIdx.x, gridDim.x);
 }
 
 template <int KM>
@@ -1177,15 +1265,15 @@ DRTOPK_DEV void emit_body(const FusedArgs& a, uint32_t cta, uint32_t ncta, uint3
   const unsigned lane = lane_id();
   const int wib = threadIdx.x >> 5;
   uint2* cstage = reinterpret_cast<uint2*>(s_dyn) + (size_t)wib * GATHER_STAGE;
-  // the predicted threshold: 16-bit prefix boundary holding pre_target
-  // sampled keys at or above it
-  const Pick p0 = block_pick<false>(a.pre_hist, 256, a.pre_target);
-  const uint32_t r1 = a.pre_target > p0.above ? a.pre_target - p0.above : 1u;
-  const Pick p1 = block_pick<false>(a.pre_hist + 256, 256, r1);
-  const uint32_t thr = ((uint32_t)p0.b << 24) | ((uint32_t)p1.b << 16);
+  // the predicted threshold: the prefix boundary (2 to 4 bytes) holding
+  // pre_target sampled keys at or above it, as the last sample pass left it
+  const uint32_t levels = ld_cg_u32(a.pre_hist + PRE_STATE + PS_DONE);
+  const uint32_t prefix = ld_cg_u32(a.pre_hist + PRE_STATE + PS_PREFIX);
+  const uint32_t thr = levels >= 4 ? prefix : (levels ? prefix << (32 - 8 * levels) : 0u);
+  if (levels == 0 && threadIdx.x == 0) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL);
   if (cta == 0 && threadIdx.x == 0) {
     *a.thr_word = thr;
-    a.stats[ST_LVA] = 2;
+    a.stats[ST_LVA] = levels;
     stamp(a.stats, 18);
   }
   // the candidates' largest key bounds level 0 of the second select
@@ -1336,11 +1424,11 @@ __global__ void __launch_bounds__(FUSED_THREADS) k_presample_g(GroupArgs g) {
 }
 
 template <int KM>
-__global__ void __launch_bounds__(FUSED_THREADS) k_presample2_g(GroupArgs g) {
+__global__ void __launch_bounds__(FUSED_THREADS) k_prerefine_g(GroupArgs g, int level) {
   __shared__ FusedArgs s_args;
   uint32_t cta, ncta;
   const FusedArgs& a = group_problem(g, &s_args, cta, ncta);
-  presample2_body<KM>(a, cta, ncta);
+  prerefine_body<KM>(a, level, cta, ncta);
 }
 
 template <int KM>

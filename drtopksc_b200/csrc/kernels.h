@@ -17,12 +17,12 @@ struct KernelSet {
   const void* split0;      // k_split0<KM>
   const void* bitonic;     // k_bitonic<KM>
   const void* presample;   // k_presample<KM>   (sampled-threshold path)
-  const void* presample2;  // k_presample2<KM>
+  const void* prerefine;   // k_prerefine<KM>   (launched per byte level 1..3)
   const void* emit;        // k_emit<KM>
   const void* cand_hist;   // k_cand_hist<KM>
   // grouped forms of the sampled-threshold path (many problems per launch)
   const void* presample_g;
-  const void* presample2_g;
+  const void* prerefine_g;
   const void* emit_g;
   const void* cand_hist_g;
   const void* split0_g;

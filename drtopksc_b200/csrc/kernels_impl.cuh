@@ -23,11 +23,11 @@ KernelSet make_kernel_set() {
   s.split0 = (const void*)k_split0<KM>;
   s.bitonic = (const void*)k_bitonic<KM>;
   s.presample = (const void*)k_presample<KM>;
-  s.presample2 = (const void*)k_presample2<KM>;
+  s.prerefine = (const void*)k_prerefine<KM>;
   s.emit = (const void*)k_emit<KM>;
   s.cand_hist = (const void*)k_cand_hist<KM>;
   s.presample_g = (const void*)k_presample_g<KM>;
-  s.presample2_g = (const void*)k_presample2_g<KM>;
+  s.prerefine_g = (const void*)k_prerefine_g<KM>;
   s.emit_g = (const void*)k_emit_g<KM>;
   s.cand_hist_g = (const void*)k_cand_hist_g<KM>;
   s.split0_g = (const void*)k_split0_g<KM>;

@@ -46,6 +46,7 @@ struct Plan {
   int split_grid, filter_grid, hist_grid, split0_grid;
   int emit_grid, presample_grid;  // sampled-threshold path
   uint32_t pre_target;            // sampled keys required at or above its predicted threshold
+  uint32_t pre_stride;            // one 512-key chunk in pre_stride is sampled
   int first_pre;       // split mode: first select in k_level_hist / k_filter (beta, radix, <= 2 levels)
   size_t fused_smem;
   size_t run_words;

@@ -98,6 +98,8 @@ typedef struct {
   int team_cluster;          /* 0: the cooperative grid; 1: one thread-block cluster; 3: one CTA
                                 (shared-memory tail); 5: one ordinary CTA */
   int kernel_launches;       /* kernels the last select launched (sampler included) */
+  int sample_stride;         /* sampled-threshold path: one 512-key chunk in sample_stride was
+                                sampled to predict the threshold (0 on the other paths) */
 } drtopk_stats_t;
 
 typedef struct drtopk_handle* drtopk_handle_t;

@@ -11,7 +11,7 @@ from tests.helpers import expected, run_topk, same_bits
 
 pytestmark = pytest.mark.gpu
 
-PRE_STRIDE = 64
+PRE_STRIDE = 64  # the planner's sampling stride for n <= 2^27 (one 512-key chunk in 64)
 
 
 def check(x, k, largest=True, offset=0, **kw):
@@ -45,12 +45,33 @@ def test_sampled_threshold_candidates_close_to_k():
     ns_keys = ((n >> 9) // PRE_STRIDE) * 512
     for k in (1 << 16, 1 << 20):
         st = check(x, k, sorted=False)
-        assert st["beta"] == 0 and st["levels_first"] == 2
+        assert st["beta"] == 0 and st["levels_first"] == 2 and st["sample_stride"] == PRE_STRIDE
         # k scaled to the sample plus the six-sigma margin, plus the sample's
         # own error in the other direction (another six sigma), plus one
         # 16-bit prefix bin of uniform keys
         ks = k * ns_keys / n
         bound = (ks + 12 * ks ** 0.5 + 32) * n / ns_keys + 2 * n / 65536
+        assert k <= st["n_candidates"] <= bound, (st, bound)
+
+
+@pytest.mark.parametrize("dist,levels", [("fewdigits", 4), ("range16", 3)])
+def test_narrow_inputs_refine_the_threshold(dist, levels):
+    # keys sharing their top 24 (few digits) or 16 bits: a 16-bit threshold
+    # would admit every key; the sample passes refine it byte by byte until
+    # the picked bin is small
+    n = 1 << 22
+    if dist == "range16":
+        x = (0x12340000 | (O.gen("u32", n, 5) & 0xFFFF)).astype(np.uint32)
+    else:
+        x = O.gen(dist, n, 5)
+    ns_keys = ((n >> 9) // PRE_STRIDE) * 512
+    for k in (16, 4096, 1 << 16):
+        st = check(x, k, sorted=False)
+        assert st["beta"] == 0 and st["levels_first"] == levels, st
+        ks = k * ns_keys / n
+        # the margin as above, plus one bin of the last refined level
+        bound = (ks + 12 * ks ** 0.5 + 32) * n / ns_keys + 2 * n / (1 << (8 * (levels - 2)))
+        bound = max(bound, 2 * n / 256)  # few digits: one value's copies
         assert k <= st["n_candidates"] <= bound, (st, bound)
 
 
@@ -87,7 +108,9 @@ def test_prediction_that_overshoots_falls_back_to_an_exact_select():
     for k in (nhigh + 1, 3 * nhigh, n // 2):
         st = check(x, k, sorted=True)
         assert st["n_candidates"] == n  # the select ran over all keys
-    st = check(x, nhigh // 2)  # the prediction holds here
+    # the sample sees only the largest keys, so it refines the threshold to
+    # their top value: the prediction holds for k up to that value's copies
+    st = check(x, nhigh // 64)
     assert st["n_candidates"] < n
 
 
