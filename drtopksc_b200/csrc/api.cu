@@ -206,6 +206,14 @@ static void* split_ptr(int km, int which) {
   }
 }
 
+// Candidates the sampled-threshold path expects: k, the six-sigma margin of
+// the key sample (in keys), and one 16-bit prefix bin of uniform keys.
+static double emit_cand_estimate(uint64_t n, uint64_t k, uint32_t stride) {
+  const double s = stride ? (double)stride : (double)PRE_STRIDE_MIN;
+  const double ks = (double)k / s;
+  return (double)k + s * (6.0 * std::sqrt(ks) + 16.0) + (double)n / 65536.0;
+}
+
 // dynamic shared memory of a split-mode kernel: histogram words + warp stages
 static size_t split_smem(int nb, int which) {
   if (which == SK_PRESAMPLE || which == SK_PREREFINE) return 0;
@@ -390,7 +398,16 @@ drtopk_status_t make_plan(uint64_t n, uint64_t k, drtopk_dtype_t dtype, const dr
   const int D = 32 / P->nbits;
   if (P->path == PATH_BETA) {
     if (P->bucket) P->first_levels = 2;  // bucketselect_combined.cuh:972-1095 (two bucket levels)
-    else P->first_levels = p.first_digits > 0 ? std::min(p.first_digits, D) : std::max(0, D - 3);
+    else if (p.first_digits == 0) P->first_levels = std::max(0, D - 3);
+    else P->first_levels = std::min(p.first_digits > 0 ? p.first_digits : -p.first_digits, D);
+    // first_digits < 0 (the autotuner's choice): at least that many digits,
+    // refined while the chosen bin still holds more than max(2k, 4096)
+    // delegates.  The tuned digit count assumes keys spread like independent
+    // uniform draws; where the delegates crowd into one bin (few distinct
+    // values, float exponents) every subrange would otherwise qualify.  The
+    // reference's digit rule (0) and explicit counts keep their digits, and
+    // the reference's counters.
+    if (p.first_digits < 0 && !P->bucket) P->adapt_first = (uint32_t)std::max<uint64_t>(2 * k, 4096);
   }
   P->fused_grid = fused_grid;
   return DRTOPK_OK;
@@ -671,8 +688,7 @@ drtopk_status_t drtopk::plan_select_bounded(int device, uint64_t n, uint64_t k, 
   if (s != DRTOPK_OK || P->path != PATH_EMIT || !P->one_cta) return s;
   // twice the expected candidates (k, the six-sigma margin, one 16-bit
   // prefix bin) plus 64K
-  const double ks = (double)k / 64.0;
-  const double est = (double)k + 64.0 * (6.0 * std::sqrt(ks) + 16.0) + (double)n / 65536.0;
+  const double est = emit_cand_estimate(n, k, P->pre_stride);
   P->bounded = 1;
   P->cap_bound = (uint64_t)(2.0 * est) + 65536;
   layout(P, want_idx);
@@ -839,6 +855,7 @@ static void fill_args(const Plan& P, const void* d_keys, void* d_kth, void* d_va
   a.alpha = P.alpha;
   a.M = P.M;
   a.first_levels = P.first_levels;
+  a.adapt_first = P.adapt_first;
   a.vec_ok = vec_ok;
   a.del_minmax = cw + CW_DEL_MINMAX;
   a.A = run_bufs(ctrl, P, 0);
@@ -855,6 +872,7 @@ static void fill_args(const Plan& P, const void* d_keys, void* d_kth, void* d_va
   a.gb.nblocks = (uint32_t)P.fused_grid;
   a.thr_word = cw + CW_THR;
   a.tail_flag = cw + CW_TAIL;
+  a.tie_cut = cw + CW_TIE_CUT;
   a.pre_hist = cw + P.pre_hist_word;
   a.pre_target = P.pre_target;
   a.pre_stride = P.pre_stride ? P.pre_stride : PRE_STRIDE_MIN;
@@ -1051,8 +1069,7 @@ size_t group_desc_bytes(int nprob) {
 // (each grouped launch covers every problem of the group)
 static uint32_t group_ctas(const Plan& P, int stage) {
   const uint64_t n = P.n, k = P.k;
-  const double ks = (double)k / 64.0;
-  const double cand = (double)k + 64.0 * (6.0 * std::sqrt(ks) + 16.0) + (double)n / 65536.0;
+  const double cand = emit_cand_estimate(n, k, P.pre_stride);
   auto clampc = [](uint64_t v, uint64_t cap) { return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(v, cap)); };
   switch (stage) {
     case GS_PRESAMPLE:
@@ -1214,7 +1231,7 @@ extern "C" drtopk_status_t drtopk_sync_check(drtopk_handle_t h, void* stream) {
 // kernels one select of plan P launches (enqueue_select's launch sequence)
 static int plan_launches(const Plan& P) {
   // k_presample, k_prerefine x 3, k_emit, k_cand_hist, k_split0, k_fused
-  if (P.path == PATH_EMIT) return 5 + PRE_LEVELS;
+  if (P.path == PATH_EMIT) return PRE_LEVELS + 4;
   const bool sampler = P.path != PATH_PLAIN && !(P.path == PATH_BITONIC && P.normal);
   int n = sampler ? 1 : 0;
   if (P.path == PATH_BITONIC || P.tail || P.cluster > 0 || !P.split) return n + 1;
@@ -1453,7 +1470,7 @@ extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_
   p->path = best_path;
   if (best_path == 2) {
     p->beta = 2;
-    if (p->nbits == 8) p->first_digits = best_digits;
+    if (p->nbits == 8) p->first_digits = -best_digits;  // at least best_digits, refined while crowded
   }
   return DRTOPK_OK;
 }

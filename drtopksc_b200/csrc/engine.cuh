@@ -41,6 +41,8 @@ struct EngineCfg {
   int thr_only;        // only the final range is wanted (histogram passes, no appends)
   int key_from_payload;  // key = ~payload (fill by lowest payload)
   int skip_split0;     // level 0's split (top list, next set, level-1 histogram) was made by another kernel
+  uint32_t adapt_cnt;  // thr_only: after max_levels, keep refining while the chosen bin holds more
+                       // than adapt_cnt entries (0: stop at max_levels)
 };
 
 struct RunBufs {
@@ -79,6 +81,7 @@ struct Src {
 
 struct RunResult {
   uint32_t thr;     // final range lower bound
+  uint32_t thr_hi;  // ... and upper bound (thr_only runs)
   uint32_t kth;     // exact k-th key when the run finished (collapse/single)
   int levels;
   int ok;
@@ -165,7 +168,8 @@ DRTOPK_DEV bool advance(const EngineCfg& c, const Level& L, const Pick& p, int l
     N.wshift = L.wshift - c.nbits;
     N.w = N.wshift >= 0 ? (1u << N.wshift) : 1u;
   }
-  bool done = (N.lo == N.hi) || (c.stop_single && p.cnt == 1) || (level_index + 1 >= c.max_levels);
+  bool done = (N.lo == N.hi) || (c.stop_single && p.cnt == 1) ||
+              (level_index + 1 >= c.max_levels && !(c.adapt_cnt && p.cnt > c.adapt_cnt));
   return done;
 }
 
@@ -769,7 +773,7 @@ template <int KM>
 DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_pairs, const RunBufs& rb,
                                 const RunBufs& fb, Level L0, uint32_t* s_hist, const Team& tm,
                                 uint2* s_fast = nullptr) {
-  RunResult res = {0u, 0u, 0, 1};
+  RunResult res = {0u, 0u, 0u, 0, 1};
   const bool can_small = s_fast && !c.thr_only && !c.key_from_payload;
   auto finish_small = [&](const Src& s, bool pairs, uint32_t cnt, const Level& L, int j0) {
     if (tm.rank == 0) block_finish<KM>(c, s, pairs, cnt, L, j0, rb, s_hist, s_fast, s_fast + SMALL_SET);
@@ -794,6 +798,7 @@ DRTOPK_DEV RunResult run_select(const EngineCfg& c, const Src& src0, bool src0_p
   int j = run_levels<KM>(c, src0, src0_pairs, rb, L0, s_hist, tm, Lf, lp, eqb, E, ok, can_small, &small);
   res.levels = j + 1;
   res.thr = Lf.lo;
+  res.thr_hi = Lf.hi;
   if (!ok) { res.ok = 0; return res; }
   if (c.thr_only) return res;
   if (small) {

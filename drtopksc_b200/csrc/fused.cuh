@@ -67,6 +67,7 @@ struct FusedArgs {
   uint32_t* stats;        // [16]
   uint32_t* thr_word;     // threshold handed between launches in split mode
   uint32_t* tail_flag;    // shared-memory tail: 1 done, 2 fall back to the general path
+  uint32_t* tie_cut;      // beta path: id bound of the subranges tied at a one-value threshold kept
   int phase_lo, phase_hi; // phases run by this launch of k_fused (1..3)
   int first_pre;          // split mode: the first select runs in k_level_hist / k_filter
   int split0;             // split mode: level 0 of the second select runs in k_split0
@@ -75,6 +76,8 @@ struct FusedArgs {
   uint32_t pre_target;    // sampled keys that must lie at or above the predicted threshold
   uint32_t pre_stride;    // one 512-key chunk in pre_stride is sampled (a power of two)
   int bounded;            // candidate buffers sized by the sample's estimate: no device fallback
+  uint32_t adapt_first;   // beta path (autotuned): the threshold-only first select keeps refining
+                          // past first_levels while its chosen bin holds more delegates than this
   GridBar gb;
 };
 
@@ -162,14 +165,95 @@ DRTOPK_DEV void gather_list(const Team& tm, const FusedArgs& a, const uint2* ids
   }
 }
 
+constexpr int FILTER_E = 8;  // subranges per thread per tile of the beta filter
+
+// Exclusive prefix sum of v over the block (all threads), with the total.
+DRTOPK_DEV uint32_t block_excl_scan(uint32_t v, uint32_t& total) {
+  __shared__ uint32_t s_w[MAX_BLOCK_WARPS];
+  const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+    if ((int)lane >= off) x += y;
+  }
+  if (lane == 31) s_w[wid] = x;
+  __syncthreads();
+  uint32_t before = 0;
+  total = 0;
+  for (unsigned w = 0; w < nw; ++w) {
+    if (w < wid) before += s_w[w];
+    total += s_w[w];
+  }
+  __syncthreads();
+  return before + x - v;
+}
+
+// Ties at a one-value threshold (the autotuned beta path's first select
+// collapsed to the single value thr, as few-digit keys make it): every
+// subrange whose Max equals thr holds copies of thr and nothing above it.
+// The k-th largest key K is >= thr.  If K > thr those subranges hold no key
+// of the top k; if K == thr, the lowest-index copies of thr the top k needs
+// lie in subranges kept whole anyway (Max > thr, Second >= thr) or in the k
+// lowest-id subranges with Max == thr, since each of those holds a copy
+// with a lower index than any copy further on.  Returns the id bound
+// (exclusive) of the tied subranges to keep: after the k-th one, or M.
+// Scratch: one word per tile of blockDim * FILTER_E subranges.
+DRTOPK_DEV uint32_t beta_tie_cut(const Team& tm, const FusedArgs& a, uint32_t thr, uint32_t* scratch) {
+  const uint64_t T = (uint64_t)blockDim.x * FILTER_E;
+  const uint64_t tiles = (a.M + T - 1) / T;
+  uint32_t tot = 0;
+  for (uint64_t t = tm.rank; t < tiles; t += tm.size) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int q = 0; q < FILTER_E; ++q) {
+      const uint64_t j = t * T + (uint64_t)q * blockDim.x + threadIdx.x;
+      if (j < a.M && a.del[2 * j] == thr) ++c;
+    }
+    block_excl_scan(c, tot);
+    if (threadIdx.x == 0) scratch[t] = tot;
+  }
+  if (!team_sync(tm)) return (uint32_t)a.M;
+  if (tm.rank == 0) {
+    __shared__ uint32_t s_found, s_tile, s_rem, s_cut;
+    if (threadIdx.x == 0) { s_found = 0; s_cut = (uint32_t)a.M; }
+    __syncthreads();
+    // the tile holding the k-th tied subrange (tiles in id order)
+    uint32_t base = 0;
+    for (uint64_t t0 = 0; t0 < tiles; t0 += blockDim.x) {
+      const uint64_t t = t0 + threadIdx.x;
+      const uint32_t v = t < tiles ? ld_cg_u32(scratch + t) : 0u;
+      const uint32_t ex = base + block_excl_scan(v, tot);
+      if (v && ex < a.k && ex + v >= a.k) { s_found = 1; s_tile = (uint32_t)t; s_rem = a.k - ex; }
+      base += tot;
+      __syncthreads();
+      if (s_found) break;
+    }
+    if (s_found) {
+      // inside it, the s_rem-th tied subrange in id order
+      uint32_t run = 0;
+      for (int q = 0; q < FILTER_E; ++q) {
+        const uint64_t j = (uint64_t)s_tile * T + (uint64_t)q * blockDim.x + threadIdx.x;
+        const uint32_t f = (j < a.M && a.del[2 * j] == thr) ? 1u : 0u;
+        const uint32_t ex = run + block_excl_scan(f, tot);
+        if (f && ex + 1 == s_rem) s_cut = (uint32_t)(j + 1);
+        run += tot;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *a.tie_cut = s_cut;
+  }
+  if (!team_sync(tm)) return (uint32_t)a.M;
+  return ld_cg_u32(a.tie_cut);
+}
+
 // beta path filter (FindTopKRanges_beta, radixselect.cuh:560-598): per
 // subrange, Max >= thr and Second >= thr -> subrange id to the selected
 // list; Max >= thr only -> Max itself is a candidate (with its position).
-constexpr int FILTER_E = 8;
-
+// Subranges whose Max equals thr with an id at or past `cut` are dropped.
 template <int KM>
 DRTOPK_DEV void filter_beta(const Team& tm, const FusedArgs& a, uint32_t thr, uint32_t* s_hist, uint32_t& mlo,
-                            uint32_t& mhi, bool& ovf) {
+                            uint32_t& mhi, bool& ovf, uint64_t cut = ~0ull) {
   const uint64_t T = (uint64_t)blockDim.x * FILTER_E;
   const int hsh = cand_shift(thr, a.nbits);
   for (uint64_t tb = (uint64_t)tm.rank * T; tb < a.M; tb += (uint64_t)tm.size * T) {
@@ -182,8 +266,9 @@ DRTOPK_DEV void filter_beta(const Team& tm, const FusedArgs& a, uint32_t thr, ui
       if (j < a.M) {
         const uint2 d = *reinterpret_cast<const uint2*>(a.del + 2 * j);
         m1[q] = d.x;
-        const bool s1 = d.x >= thr && d.y >= thr;
-        const bool l1 = d.x >= thr && d.y < thr;
+        const bool keep = d.x != thr || j < cut;  // tied subranges past the cut hold no needed key
+        const bool s1 = keep && d.x >= thr && d.y >= thr;
+        const bool l1 = keep && d.x >= thr && d.y < thr;
         sel |= (uint32_t)s1 << q;
         lon |= (uint32_t)l1 << q;
         cs += s1;
@@ -370,6 +455,7 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
   const int D = 32 / a.nbits;
   uint32_t thr1 = 0, nsel = 0, nlonely = 0;
   int lvA = 0;
+  bool thr_one = false;  // the threshold-only first select ended on a single value
   if (lead && a.phase_lo <= 1) stamp(a.stats, 16);
 
   // ---------------- phase 1: first select on the delegates
@@ -388,7 +474,7 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
     } else {
       L0 = radix_level0(a.nbits, a.k);
     }
-    EngineCfg c;
+    EngineCfg c = {};
     c.bucket = a.bucket; c.nbits = a.nbits; c.nb = a.nb; c.key_from_payload = 0;
     if (a.path == PATH_DEFAULT) {
       c.stop_single = 1; c.thr_only = 0;
@@ -396,6 +482,7 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
     } else {
       c.stop_single = 0; c.thr_only = 1;
       c.max_levels = a.first_levels;
+      c.adapt_cnt = a.adapt_first;
     }
     if (a.path == PATH_BETA && c.max_levels <= 0) {
       thr1 = 0;  // no digit processed: every subrange qualifies
@@ -403,6 +490,7 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
       RunResult r = run_select<KM>(c, s, false, a.A, a.AF, L0, s_hist, tm, s_fast);
       if (!r.ok) { if (lead) atomicOr(a.gb.err, (uint32_t)DE_INTERNAL); return; }
       lvA = r.levels;
+      thr_one = c.thr_only && r.thr_hi == r.thr;
       // radix keeps the reference's flag (final range lower bound); the bucket
       // variant uses the exact k-th delegate on its default path
       thr1 = (a.path == PATH_DEFAULT && a.bucket) ? r.kth : r.thr;
@@ -434,7 +522,13 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
     }
     gather_list<KM>(tm, a, a.A.top, nullptr, a.k, thr1, s_hist, mlo, mhi, ovf);
   } else if (a.path == PATH_BETA) {
-    filter_beta<KM>(tm, a, thr1, s_hist, mlo, mhi, ovf);
+    // autotuned select whose threshold collapsed to one value: keep only
+    // the k lowest-id subranges tied at it (scratch: the second run's
+    // compact buffer, unused until phase 3)
+    const uint64_t cut = (a.adapt_first && !a.bucket && thr_one)
+                             ? (uint64_t)beta_tie_cut(tm, a, thr1, reinterpret_cast<uint32_t*>(a.C.cbuf[0]))
+                             : ~0ull;
+    filter_beta<KM>(tm, a, thr1, s_hist, mlo, mhi, ovf, cut);
     if (!team_sync(tm)) return;
     const uint32_t nsel_sub = ld_cg_u32(a.sel_count);
     if (lead) {
@@ -516,13 +610,14 @@ DRTOPK_DEV void fused_body(const FusedArgs& a, const Team& tm, uint32_t* s_dyn) 
     if (!team_sync(tm)) return;
   } else {
     // candidates of the sampled paths are all >= thr1 (their level-0
-    // histogram was built against this level by the concatenation)
+    // histogram was built against this level by the concatenation, or by
+    // k_cand_hist)
     L0c = (a.path == PATH_PLAIN || emit_fb)
               ? radix_level0(a.nbits, a.k)
               : (a.path == PATH_EMIT ? cand_level0_tight(thr1, ld_cg_u32(a.cand_minmax + 1), a.nbits, a.k)
                                      : cand_level0(thr1, a.nbits, a.k));
   }
-  EngineCfg cc;
+  EngineCfg cc = {};
   cc.bucket = a.bucket; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
   cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0; cc.skip_split0 = emit_fb ? 0 : a.split0;
   // entries k_split0 already wrote to the output (slots [0, c0) of the list)
@@ -736,7 +831,7 @@ DRTOPK_DEV void hist_add_conv(uint32_t* h, bool in, uint32_t bin) {
 // the delegate histograms A.H[0] (sampler) and A.H[1] (k_level_hist).  Every
 // CTA computes them redundantly; `upto` levels are picked.
 DRTOPK_DEV Level beta_first_levels(const FusedArgs& a, int upto, int& levels) {
-  EngineCfg c;
+  EngineCfg c = {};
   c.bucket = 0; c.nbits = a.nbits; c.nb = a.nb; c.stop_single = 0; c.thr_only = 1;
   c.max_levels = a.first_levels; c.key_from_payload = 0;
   Level L = radix_level0(a.nbits, a.k);
@@ -813,7 +908,7 @@ DRTOPK_DEV void split0_body(const FusedArgs& a, uint32_t cta, uint32_t ncta, uin
   const uint32_t thr = ld_cg_u32(a.thr_word);
   const uint32_t ncand = ld_cg_u32(a.cand_count);
   if (ncand < a.k || ncand > a.cand_cap) return;  // uniform; the second select reports it
-  EngineCfg cc;
+  EngineCfg cc = {};
   cc.bucket = 0; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
   cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0; cc.skip_split0 = 0;
   const Level L0 = a.path == PATH_EMIT ? cand_level0_tight(thr, ld_cg_u32(a.cand_minmax + 1), a.nbits, a.k)
@@ -1085,10 +1180,12 @@ constexpr uint64_t PRE_SAMPLE_CHUNKS = 4096;
 constexpr int PRE_ROUND = 4;     // sampled chunks in flight per warp
 constexpr int PRE_CTAS_PER_SM = 2;
 constexpr int PRE_LEVELS = 4;    // byte levels of the predicted threshold (at least 2 are used)
-// a picked bin holding more keys than this (estimated from the sample) is
-// refined by one more sample pass: one pass over the L2-resident sample
-// costs about what appending this many extra candidates does
-constexpr uint64_t PRE_REFINE_KEYS = 1ull << 20;
+// a picked bin holding more keys (estimated from the sample) than
+// max(PRE_REFINE_KEYS, k / 4) is refined by one more sample pass: one pass
+// over the L2-resident sample costs a few microseconds, about what
+// appending and selecting over this many extra candidates does (float keys,
+// whose top bytes are sign and exponent, and few-digit keys need it)
+constexpr uint64_t PRE_REFINE_KEYS = 1ull << 16;
 // control words after the PRE_LEVELS histograms (pre_hist + PRE_STATE):
 // [0, PRE_LEVELS) CTAs done per level, then the walk's state
 constexpr int PRE_STATE = 256 * PRE_LEVELS;
@@ -1129,7 +1226,8 @@ DRTOPK_DEV void pre_publish(const FusedArgs& a, int level, uint32_t ncta) {
     const Pick p = block_pick<false>(a.pre_hist + 256 * l, 256, r);
     prefix = (prefix << 8) | p.b;
     r = r > p.above ? r - p.above : 1u;
-    if (l >= 1 && (l == PRE_LEVELS - 1 || (uint64_t)p.cnt * a.pre_stride <= PRE_REFINE_KEYS)) {
+    if (l >= 1 && (l == PRE_LEVELS - 1 ||
+                   (uint64_t)p.cnt * a.pre_stride <= max(PRE_REFINE_KEYS, (uint64_t)a.k / 4))) {
       done = l + 1;
       break;
     }

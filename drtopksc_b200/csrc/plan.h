@@ -21,6 +21,7 @@ enum CtrlWord : int {
   CW_SEL_COUNT = 9,
   CW_THR = 10,         // first-select threshold handed between launches
   CW_TAIL = 11,        // shared-memory tail outcome
+  CW_TIE_CUT = 12,     // beta path, ties at a one-value threshold: subrange-id bound of the tied ones kept
   CW_STATS = 16,       // 32 words
   CTRL_HDR_WORDS = 48
 };
@@ -41,6 +42,8 @@ struct Plan {
   int cluster;         // > 0: phases after the sampler run in one thread-block cluster of this many CTAs
   int tail;            // 1: phases after the sampler run in one CTA with the sets in shared memory
   int one_cta;         // sampled-threshold path: the last levels run in one ordinary CTA (no co-residency)
+  uint32_t adapt_first;  // autotuned beta path: the first select refines past first_levels while its
+                         // chosen bin holds more delegates than this (0: the reference's digits)
   int bounded;         // ... with candidate buffers of cap_bound entries (served form; DE_RETRY on overflow)
   uint64_t cap_bound;
   int split_grid, filter_grid, hist_grid, split0_grid;

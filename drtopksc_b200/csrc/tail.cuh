@@ -163,10 +163,10 @@ DRTOPK_DEV bool tail_small(const FusedArgs& a, uint32_t* s_dyn) {
                        [&](uint32_t i, uint32_t v) { sA[i] = make_uint2(v, i); });
     __syncthreads();
     n = Md;
-    EngineCfg c;
+    EngineCfg c = {};
     c.bucket = 0; c.nbits = a.nbits; c.nb = a.nb; c.key_from_payload = 0;
     if (a.path == PATH_DEFAULT) { c.stop_single = 1; c.thr_only = 0; c.max_levels = D; }
-    else { c.stop_single = 0; c.thr_only = 1; c.max_levels = a.first_levels; }
+    else { c.stop_single = 0; c.thr_only = 1; c.max_levels = a.first_levels; c.adapt_cnt = a.adapt_first; }
     if (!(a.path == PATH_BETA && c.max_levels <= 0)) {
       Level L = radix_level0(a.nbits, a.k);
       int j = 0;
@@ -245,7 +245,7 @@ DRTOPK_DEV bool tail_small(const FusedArgs& a, uint32_t* s_dyn) {
     __syncthreads();
     if (lead) s_ntop = 0;
     __syncthreads();
-    EngineCfg cc;
+    EngineCfg cc = {};
     cc.bucket = 0; cc.nbits = a.nbits; cc.nb = a.nb; cc.stop_single = 1;
     cc.max_levels = MAX_LEVELS; cc.thr_only = 0; cc.key_from_payload = 0;
     Level L = cand_level0(thr1, a.nbits, a.k);  // every candidate is >= thr1 (0 on the plain path)

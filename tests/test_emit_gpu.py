@@ -46,6 +46,8 @@ def test_sampled_threshold_candidates_close_to_k():
     for k in (1 << 16, 1 << 20):
         st = check(x, k, sorted=False)
         assert st["beta"] == 0 and st["levels_first"] == 2 and st["sample_stride"] == PRE_STRIDE
+        # sample passes (4), the appending pass, k_cand_hist, k_split0, k_fused
+        assert st["kernel_launches"] == 8, st
         # k scaled to the sample plus the six-sigma margin, plus the sample's
         # own error in the other direction (another six sigma), plus one
         # 16-bit prefix bin of uniform keys
@@ -115,6 +117,8 @@ def test_prediction_that_overshoots_falls_back_to_an_exact_select():
 
 
 def test_heavy_ties_and_constant_input():
+    # every key ties: the threshold refines to the tied value itself
     for x in (np.full(1 << 20, 9, dtype=np.uint32), np.repeat(np.arange(64, dtype=np.uint32), 1 << 14)):
         for k in (1, 1000, x.size // 2, x.size):
             check(x, k)
+            check(x, k, sorted=False)

@@ -84,6 +84,41 @@ def test_beta_first_digits(fd):
         check_exact(x, k, alpha=4, path=2, first_digits=fd)
 
 
+@pytest.mark.parametrize("dist", ["fewdigits", "f32u"])
+def test_tuned_beta_threshold_refines_crowded_bins(dist):
+    # first_digits < 0 (the autotuner's form): at least that many digits,
+    # more while the chosen bin holds more than max(2k, 4096) delegates --
+    # few-digit keys share 24 bits and float keys their exponent, so a
+    # 16-bit threshold would make every subrange qualify
+    n = 1 << 22
+    x = O.gen(dist, n, 11)
+    for k in (16, 3000):
+        st = check_exact(x, k, alpha=8, path=2, first_digits=-2)
+        assert st["levels_first"] >= 3, st
+        assert st["n_candidates"] <= max(4 * k, n // 128), st
+        if dist == "fewdigits":  # the threshold is one value: only k tied subranges are read
+            assert st["n_selected"] + st["n_lonely"] <= k, st
+    # explicit digit counts keep exactly their digits
+    st = check_exact(x, 16, alpha=8, path=2, first_digits=2)
+    assert st["levels_first"] == 2, st
+
+
+def test_tied_subranges_cut_keeps_the_lowest_index_copies():
+    # few-digit keys with larger keys planted: the threshold collapses to the
+    # top few-digit value t; subranges with a planted Max and Second >= t are
+    # read whole, of those with Max == t only the k lowest-id ones -- the top
+    # k (planted keys, then the lowest-index copies of t) must be exact
+    n = 1 << 20
+    x = O.gen("fewdigits", n, 21)
+    rng = np.random.default_rng(5)
+    for planted in (1, 100, 2000):
+        y = x.copy()
+        y[rng.choice(n, planted, replace=False)] = 0xABCE0000 + rng.integers(0, 64, planted).astype(np.uint32)
+        for k in (planted, planted + 1, planted + 300, 5000):
+            for alpha in (6, 8, 10):
+                check_exact(y, k, alpha=alpha, path=2, first_digits=-1)
+
+
 @pytest.mark.parametrize("nb", [2, 16, 256, 1000, 4096])
 def test_bucket_variant_exact(nb):
     for dist in ("u32", "normal", "fewdigits", "f32n"):
