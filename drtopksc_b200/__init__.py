@@ -107,6 +107,8 @@ def lib() -> ctypes.CDLL:
             "drtopk_select_noalloc": (st, [vp, i32, u64, u64, P(Params), vp, vp, vp, vp]),
             "drtopk_noalloc_sync_check": (st, [vp]),
             "drtopk_load_dataset": (st, [ctypes.c_char_p, i32, u64, P(ctypes.c_uint32), P(ctypes.c_uint64)]),
+            "drtopk_bmw_select": (st, [vp, vp, P(ctypes.c_uint32), u64, u64, i32, P(ctypes.c_uint32),
+                                       P(ctypes.c_uint64), P(ctypes.c_double), P(ctypes.c_double)]),
             "drtopk_sync_check": (st, [vp, vp]),
             "drtopk_last_stats": (st, [vp, P(Stats)]),
             "drtopk_autotune": (st, [u64, u64, i32, P(Params)]),
@@ -250,6 +252,19 @@ class Handle:
                    idx_ptr=None, stream=None):
         check(lib().drtopk_select(self._h, keys_ptr, dtype, n, k, ctypes.byref(p), kth_ptr, vals_ptr, idx_ptr,
                                   stream), "drtopk_select")
+
+    def bmw_select(self, d_keys, h_keys, k: int, alpha: int):
+        """BMW experiment (drtopk_bmw_select): device delegates, host heap scan
+        with delegate skipping over h_keys (numpy uint32, the same keys as the
+        CUDA tensor d_keys).  Returns (kth, keys skipped, ms sample, ms scan)."""
+        import numpy as np
+        hk = np.ascontiguousarray(h_keys, dtype=np.uint32)
+        kth, sk = ctypes.c_uint32(0), ctypes.c_uint64(0)
+        m1, m2 = ctypes.c_double(0), ctypes.c_double(0)
+        check(lib().drtopk_bmw_select(self._h, d_keys.data_ptr(), hk.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                      hk.size, k, alpha, ctypes.byref(kth), ctypes.byref(sk), ctypes.byref(m1),
+                                      ctypes.byref(m2)), "drtopk_bmw_select")
+        return kth.value, sk.value, m1.value, m2.value
 
     def sync_check(self, stream=None):
         check(lib().drtopk_sync_check(self._h, _stream_ptr(stream)), "drtopk_sync_check")

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -1225,6 +1226,85 @@ extern "C" drtopk_status_t drtopk_sync_check(drtopk_handle_t h, void* stream) {
     if (s == DRTOPK_OK) s = device_error_status(hdr[CW_ERR]);
   }
   cudaSetDevice(cur);
+  return s;
+}
+
+// BMW: device delegates, then the host heap scan that skips subranges whose
+// Max is below the heap's minimum once the heap holds k keys (the
+// reference's threshold applies from the first push on, which can drop keys
+// the answer needs while the heap is not yet full; here it applies once the
+// heap is full, so the k-th is exact)
+extern "C" drtopk_status_t drtopk_bmw_select(drtopk_handle_t h, const void* d_keys, const uint32_t* h_keys, uint64_t n,
+                                             uint64_t k, int alpha, uint32_t* kth, uint64_t* n_skipped,
+                                             double* ms_sample, double* ms_scan) {
+  if (!h || !d_keys || !h_keys || !kth || n == 0 || k < 1 || k > n || alpha < 1 || alpha > 24)
+    return DRTOPK_EINVAL;
+  std::lock_guard<std::mutex> lk(h->mu);
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != h->device) cudaSetDevice(h->device);
+  drtopk_params_t p;
+  drtopk_params_default(&p);
+  p.alpha = alpha;
+  p.path = 1;
+  Plan P;
+  const uint64_t M = (n + (1ull << alpha) - 1) >> alpha;
+  drtopk_status_t s = M < k ? DRTOPK_EINVAL : plan_for(h->device, n, k, DRTOPK_U32, &p, false, &P, nullptr);
+  if (s == DRTOPK_OK) s = ensure_ws(h, P.ws_bytes);
+  std::vector<uint32_t> del;
+  const auto t0 = std::chrono::steady_clock::now();
+  if (s == DRTOPK_OK) {
+    char* ws = static_cast<char*>(h->ws);
+    uint32_t* cw = reinterpret_cast<uint32_t*>(ws + P.off_ctrl);
+    SampleArgs sa;
+    std::memset(&sa, 0, sizeof(sa));
+    sa.keys = static_cast<const uint32_t*>(d_keys);
+    sa.n = n;
+    sa.alpha = alpha;
+    sa.nbits = 8;
+    sa.hmode = 0;
+    sa.vec_ok = (reinterpret_cast<uintptr_t>(d_keys) & 15u) == 0;
+    sa.del = reinterpret_cast<uint32_t*>(ws + P.off_del);
+    sa.err = cw + CW_ERR;
+    del.resize(M);
+    if (cudaMemsetAsync(cw, 0, P.ctrl_bytes, nullptr) != cudaSuccess ||
+        launch_sampler_km(P, sa, 1, nullptr) != cudaSuccess ||
+        cudaMemcpy(del.data(), sa.del, M * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+      s = DRTOPK_ECUDA;
+  }
+  const auto t1 = std::chrono::steady_clock::now();
+  if (s == DRTOPK_OK) {
+    const uint64_t S = 1ull << alpha;
+    std::vector<uint32_t> heap;  // min-heap of the k largest keys seen
+    heap.reserve((size_t)k + 1);
+    const auto gt = std::greater<uint32_t>();
+    uint64_t skip = 0;
+    for (uint64_t j = 0; j < M; ++j) {
+      const uint64_t b = j * S, e = std::min(n, b + S);
+      if (heap.size() == (size_t)k && del[j] < heap.front()) {
+        skip += e - b;
+        continue;
+      }
+      uint64_t i = b;
+      for (; i < e && heap.size() < (size_t)k; ++i) {
+        heap.push_back(h_keys[i]);
+        std::push_heap(heap.begin(), heap.end(), gt);
+      }
+      for (; i < e; ++i) {
+        if (h_keys[i] > heap.front()) {
+          std::pop_heap(heap.begin(), heap.end(), gt);
+          heap.back() = h_keys[i];
+          std::push_heap(heap.begin(), heap.end(), gt);
+        }
+      }
+    }
+    *kth = heap.front();
+    if (n_skipped) *n_skipped = skip;
+  }
+  const auto t2 = std::chrono::steady_clock::now();
+  if (ms_sample) *ms_sample = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  if (ms_scan) *ms_scan = std::chrono::duration<double, std::milli>(t2 - t1).count();
+  if (cur != h->device) cudaSetDevice(cur);
   return s;
 }
 

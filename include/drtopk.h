@@ -259,6 +259,18 @@ typedef enum {
 DRTOPK_API drtopk_status_t drtopk_load_dataset(const char* path, int format, uint64_t n, uint32_t* h_keys,
                                                uint64_t* n_read);
 
+/* BMW experiment (replaces BMW/radixselect.cuh:1746-1832 with BMW/PQ.h):
+ * the device sampler writes one delegate (Max) per subrange of 2^alpha keys
+ * of d_keys; the host then scans h_keys (the same n uint32 keys) in order,
+ * keeping the k largest seen in a min-heap, and skips every subrange whose
+ * Max is below the heap's minimum once the heap holds k keys.  *kth: the
+ * k-th largest key (exact); *n_skipped: keys the scan never examined (the
+ * reference's NSkipDocument); *ms_sample, *ms_scan (any may be NULL): the
+ * sampler with its copy to the host, and the scan.  Blocking. */
+DRTOPK_API drtopk_status_t drtopk_bmw_select(drtopk_handle_t h, const void* d_keys, const uint32_t* h_keys,
+                                             uint64_t n, uint64_t k, int alpha, uint32_t* kth,
+                                             uint64_t* n_skipped, double* ms_sample, double* ms_scan);
+
 /* ---------------------------------------------------------------------
  * Batched form: many independent top-k problems in one persistent launch.
  * Segment s covers keys[offsets[s] .. offsets[s+1]) of one dtype; its k is

@@ -21,6 +21,7 @@
 // order-preserving map of oracle_f32_to_key.
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -510,6 +511,46 @@ int oracle_bitonic_topk(const uint32_t* x, uint64_t n, int64_t k, int alpha, uin
     if (idx) idx[i] = (int64_t)c[i].second;
   }
   return 0;
+}
+
+// BMW experiment (BMW/radixselect.cuh:1746-1832 with the min-heap of
+// BMW/PQ.h): one delegate (Max) per subrange of 2^alpha keys, then one
+// sequential scan that keeps the k largest keys seen in a min-heap; once the
+// heap holds k keys its minimum is the threshold, a key enters only above it
+// (evicting the minimum), and a subrange whose Max is below the threshold is
+// skipped whole.  The reference makes the heap's minimum the threshold from
+// the first push on, so while the heap is not yet full it can drop keys the
+// answer needs; here the threshold applies once the heap is full, which
+// keeps the k-th exact.  Returns the k-th largest key; *skipped counts the
+// keys never examined.
+uint32_t oracle_bmw_kth(const uint32_t* x, uint64_t n, int64_t k, int alpha, uint64_t* skipped) {
+  const uint64_t S = 1ull << alpha, M = (n + S - 1) / S;
+  std::vector<uint32_t> del(M);
+  oracle_sample_max(x, n, alpha, del.data());
+  std::vector<uint32_t> heap;  // min-heap
+  heap.reserve((size_t)k + 1);
+  auto gt = std::greater<uint32_t>();
+  uint64_t skip = 0;
+  for (uint64_t j = 0; j < M; ++j) {
+    const uint64_t b = j * S, e = std::min(n, b + S);
+    const bool full = heap.size() == (size_t)k;
+    if (full && del[j] < heap.front()) {
+      skip += e - b;
+      continue;
+    }
+    for (uint64_t i = b; i < e; ++i) {
+      if (heap.size() < (size_t)k) {
+        heap.push_back(x[i]);
+        std::push_heap(heap.begin(), heap.end(), gt);
+      } else if (x[i] > heap.front()) {
+        std::pop_heap(heap.begin(), heap.end(), gt);
+        heap.back() = x[i];
+        std::push_heap(heap.begin(), heap.end(), gt);
+      }
+    }
+  }
+  if (skipped) *skipped = skip;
+  return heap.front();
 }
 
 // FNV-1a over the sorted top-k (values then indices): a compact fixture digest.

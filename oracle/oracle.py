@@ -70,6 +70,7 @@ def lib():
             "oracle_bucket_kth": (i32, [u32p, u64, i64, i32, i32, i32, u32p, ctypes.POINTER(OracleStats)]),
             "oracle_bitonic_topk": (i32, [u32p, u64, i64, i32, u32p, i64p]),
             "oracle_digest": (ctypes.c_uint64, [u32p, i64p, i64]),
+            "oracle_bmw_kth": (u32, [u32p, u64, i64, i32, ctypes.POINTER(ctypes.c_uint64)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -206,6 +207,15 @@ def topk_mt(x: np.ndarray, k: int, threads: int):
     sec = lib().oracle_topk_mt(_p(x, ctypes.c_uint32), x.size, k, threads, ctypes.byref(kth),
                                _p(vals, ctypes.c_uint32))
     return sec, kth.value, vals
+
+
+def bmw_kth(x: np.ndarray, k: int, alpha: int):
+    """The BMW experiment's heap scan with delegate skipping
+    (BMW/radixselect.cuh:1746-1832): (k-th largest key, keys skipped)."""
+    x = np.ascontiguousarray(x, dtype=np.uint32)
+    sk = ctypes.c_uint64(0)
+    kth = lib().oracle_bmw_kth(_p(x, ctypes.c_uint32), x.size, k, alpha, ctypes.byref(sk))
+    return int(kth), int(sk.value)
 
 
 def digest(vals: np.ndarray, idx: np.ndarray | None = None) -> int:

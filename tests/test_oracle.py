@@ -96,3 +96,18 @@ def test_oracle_matches_reference_golden_kth():
             assert not reference_counters_match(O.as_keys(x), c, got, c["alpha"], c["k"]), (c, got)
         checked += 1
     assert checked >= 20
+
+
+def test_bmw_scan_is_exact_and_skips():
+    # the BMW heap scan (threshold active once the heap holds k keys) gives
+    # the exact k-th; on uniform keys most subranges are skipped
+    for dist in ("u32", "normal", "fewdigits"):
+        x = O.gen(dist, 1 << 16, 3)
+        for k in (1, 10, 700):
+            for alpha in (4, 8):
+                kth, sk = O.bmw_kth(x, k, alpha)
+                ek = O.topk_exact(x, k, want_topk=False)[0]
+                assert kth == ek, (dist, k, alpha)
+                assert 0 <= sk < x.size
+    kth, sk = O.bmw_kth(O.gen("u32", 1 << 16, 4), 5, 8)
+    assert sk > (1 << 15)
