@@ -542,7 +542,7 @@ def main():
     ap.add_argument("--batch-segments", type=int, default=4096)
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-pool", type=int, default=48)
-    ap.add_argument("--serve-inflight", type=int, default=128, help="server in-flight request limit")
+    ap.add_argument("--serve-inflight", type=int, default=256, help="server in-flight request limit")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.5, 0.9],
                     help="offered loads (Poisson) as fractions of the server's measured saturation rate")
     args = ap.parse_args()

@@ -62,6 +62,11 @@ class Stats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class SegParams(ctypes.Structure):
+    _fields_ = [("algo", ctypes.c_int), ("alpha", ctypes.c_int), ("beta", ctypes.c_int), ("nbits", ctypes.c_int),
+                ("bucket", ctypes.c_int), ("chunk_log2", ctypes.c_int)]
+
+
 class ServerStats(ctypes.Structure):
     _fields_ = [("singles", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("batched", ctypes.c_uint64),
                 ("pinned_allocs", ctypes.c_uint64), ("worker_ticks", ctypes.c_uint64),
@@ -124,6 +129,9 @@ def lib() -> ctypes.CDLL:
             "drtopk_batch_run_graph": (st, [vp, vp, vp, vp, vp, vp]),
             "drtopk_batch_sync_check": (st, [vp, vp]),
             "drtopk_batch_describe": (st, [vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]),
+            "drtopk_batch_plan_params": (st, [vp, i32, P(ctypes.c_uint64), P(ctypes.c_uint32), P(ctypes.c_int), i32,
+                                              P(SegParams)]),
+            "drtopk_batch_describe_params": (st, [vp, P(SegParams)]),
             "drtopk_server_create": (st, [P(vp), i32, sz, i32]),
             "drtopk_server_destroy": (st, [vp]),
             "drtopk_server_submit": (st, [vp, vp, i32, u64, u64, i32, vp, vp, P(ctypes.c_uint64)]),
@@ -446,16 +454,29 @@ class Batch:
         except Exception:  # noqa: BLE001
             pass
 
-    def plan(self, offsets, ks, dtypes=None, sorted: bool = False):
+    def plan(self, offsets, ks, dtypes=None, sorted: bool = False, params=None):
+        """params: None (every knob tuned) or one dict per segment with any of
+        algo ("plain", "radix", "bitonic"), alpha, beta, nbits, bucket,
+        chunk_log2 -- the ones left out are tuned (drtopk_seg_params_t)."""
         import numpy as np
         off = np.ascontiguousarray(offsets, dtype=np.uint64)
         kk = np.ascontiguousarray(ks, dtype=np.uint32)
         nseg = kk.size
         dt = np.ascontiguousarray(dtypes if dtypes is not None else np.zeros(nseg), dtype=np.int32)
-        check(lib().drtopk_batch_plan(self._b, nseg, off.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
-                                      kk.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
-                                      dt.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(bool(sorted))),
-              "drtopk_batch_plan")
+        arr = None
+        if params is not None:
+            arr = (SegParams * nseg)()
+            for s, q in enumerate(params):
+                algo = q.get("algo", -1)
+                if isinstance(algo, str):
+                    algo = _ALGOS[algo]
+                arr[s] = SegParams(algo, q.get("alpha", -1), q.get("beta", -1), q.get("nbits", -1),
+                                   int(q.get("bucket", -1)), q.get("chunk_log2", -1))
+        check(lib().drtopk_batch_plan_params(self._b, nseg, off.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                             kk.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                             dt.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(bool(sorted)),
+                                             arr),
+              "drtopk_batch_plan_params")
         self.nseg = nseg
         self.out_offsets = np.concatenate([[0], np.cumsum(kk.astype(np.int64))])
         return self
@@ -477,6 +498,12 @@ class Batch:
         check(lib().drtopk_batch_describe(self._b, a.ctypes.data_as(P), al.ctypes.data_as(P), be.ctypes.data_as(P)),
               "drtopk_batch_describe")
         return a, al, be
+
+    def describe_params(self):
+        """The tuned knobs of every segment, as dicts (drtopk_seg_params_t)."""
+        arr = (SegParams * self.nseg)()
+        check(lib().drtopk_batch_describe_params(self._b, arr), "drtopk_batch_describe_params")
+        return [{f: getattr(q, f) for f, _ in SegParams._fields_} for q in arr]
 
 
 class Server:

@@ -56,26 +56,142 @@ namespace {
 
 inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Per-segment choice: plain block select for short segments, else the
-// delegate path with S ~ sqrt(5 len / k) (delegates are written once and
-// read ~4x from L2 by the block select; the k kept subranges are re-read).
-void choose(uint32_t len, uint32_t k, int& mode, int& alpha) {
-  if (len <= 32768) {
-    mode = SEG_PLAIN;
-    alpha = 0;
-    return;
+// ------------------------------------------------------------ autotuner
+// Per segment, the configuration with the lowest modelled cost: HBM bytes at
+// the copy bandwidth plus the select task's CTA time shared by the resident
+// CTAs.  A block pass over n entries costs SEG_T_PASS (histogram clear,
+// barriers, the pick) plus n * SEG_T_ELEM of one CTA.  The model prices every
+// knob of drtopk_seg_params_t; it has no view of the keys, so it prices
+// bucket levels as radix ones plus the min/max pass (the bucket select pays
+// off on keys of a narrow range, which a caller can ask for) and 4-bit
+// digits as twice the passes.
+// Calibrated on B200 against forced-knob runs of the 4096-segment batch
+// (lengths 2^10..2^22): a block pass is latency-bound (~2K entries per us and
+// a few us of barriers and picks); a delegate entry costs about five times a
+// candidate entry (the alpha that minimised the batch time sits at
+// 2^alpha ~ sqrt(5 len / k)) and a raw key of a plain segment about 2.5
+// (plain segments were fastest up to ~16K keys); the bitonic network of a whole segment loses
+// to the radix passes from ~1K keys up; and the beta-2 sampler's top-two
+// bookkeeping costs about as much as the keys' HBM time.
+constexpr double SEG_BW = 6.0e6;        // HBM bytes per us (whole GPU)
+constexpr double SEG_T_PASS = 4.0;      // us per block pass (one CTA)
+constexpr double SEG_T_ELEM = 0.0005;   // us per entry per pass (one CTA)
+constexpr double SEG_DEL_WEIGHT = 5.0;  // a delegate entry against a candidate entry
+constexpr double SEG_KEY_WEIGHT = 2.5;  // a raw key of a plain segment against a candidate entry
+constexpr double SEG_T_TASK = 1.0;      // us per sampler task (ticket, barriers)
+constexpr double SEG_T_SAMP = 0.0006;   // us per key sampled (one CTA)
+constexpr double SEG_T_SAMP2 = 8.6e-7;  // us of batch time per key: beta 2's top-two sampler
+constexpr double SEG_T_STAGE = 0.6;     // us per bitonic stage (one CTA, up to 4096 entries)
+
+struct SegChoice {
+  int mode, alpha, beta, nbits, sel, chunk_log2;
+  double cost;
+};
+
+double passes_of(int nbits, int sel) { return sel == SEG_BUCKET ? 1.0 + 32.0 / 8.0 : 32.0 / nbits; }
+
+// one block select (passes) + the ordered take over n entries
+double block_cost(double n, int nbits, int sel, double ctas) {
+  const double p = passes_of(nbits, sel) + 1.0;
+  return p * (SEG_T_PASS + n * SEG_T_ELEM) / ctas;
+}
+
+double sort_cost(uint32_t k, int sorted, double ctas) {
+  if (!sorted) return 0.0;
+  const double L = std::ceil(std::log2(std::max(2.0, (double)k)));
+  return L * (L + 1.0) / 2.0 * SEG_T_STAGE / ctas;
+}
+
+SegChoice cost_plain(uint32_t len, uint32_t k, int sorted, int nbits, int sel, double ctas) {
+  const double c = SEG_KEY_WEIGHT * block_cost(len, nbits, sel, ctas) + sort_cost(k, sorted, ctas);
+  return {SEG_PLAIN, 0, 0, nbits, sel, 0, c + 4.0 * len / SEG_BW};
+}
+
+SegChoice cost_bitonic(uint32_t len, double ctas) {
+  const double L = std::ceil(std::log2(std::max(2.0, (double)len)));
+  const double c = (SEG_T_PASS + len * SEG_T_ELEM + L * (L + 1.0) / 2.0 * SEG_T_STAGE) / ctas;
+  return {SEG_BITONIC, 0, 0, 8, SEG_RADIX, 0, c + 4.0 * len / SEG_BW};
+}
+
+SegChoice cost_delegate(uint32_t len, uint32_t k, int sorted, int alpha, int beta, int nbits, int sel, int chunk_log2,
+                        double ctas) {
+  const double S = std::ldexp(1.0, alpha), M = std::ceil(len / S);
+  const double tasks = std::ceil(len / std::ldexp(1.0, chunk_log2));
+  double hbm = 4.0 * len + 4.0 * M * (beta == 2 ? 3 : 1);
+  double c = (tasks * SEG_T_TASK + len * SEG_T_SAMP) / ctas + (beta == 2 ? len * SEG_T_SAMP2 : 0.0);
+  double cand;
+  if (beta == 1) {
+    c += SEG_DEL_WEIGHT * block_cost(M, nbits, sel, ctas);
+    cand = k * S;  // the k kept subranges, read whole
+    hbm += 4.0 * cand;
+  } else {
+    c += SEG_DEL_WEIGHT * block_cost(2.0 * M, nbits, sel, ctas);
+    c += (SEG_T_PASS * 3.0 + M * SEG_T_ELEM * 2.0) / ctas;  // the ordered list of kept subranges
+    // subranges holding >= 2 of the top keys are read whole, the others
+    // give their Max (keys i.i.d.: lam top keys per subrange)
+    const double lam = k * S / len;
+    const double whole = M * (1.0 - std::exp(-lam) * (1.0 + lam));
+    cand = whole * S + k;
+    hbm += 4.0 * whole * S;
+    c += cand * SEG_T_ELEM * 2.0 / ctas;  // virtual positions found by binary search
   }
-  double s = std::sqrt(5.0 * (double)len / (double)k);
-  int a = (int)std::lround(std::log2(std::max(2.0, s)));
-  a = std::max(5, std::min(a, 15));
-  while (a > 5 && ((((uint64_t)len + (1ull << a) - 1) >> a) < k)) a--;
-  if ((((uint64_t)len + (1ull << a) - 1) >> a) < k) {
-    mode = SEG_PLAIN;
-    alpha = 0;
-    return;
+  c += (SEG_T_PASS + cand * SEG_T_ELEM) / ctas;  // concatenation
+  c += block_cost(cand, nbits, sel, ctas) + sort_cost(k, sorted, ctas);
+  return {SEG_DELEGATE, alpha, beta, nbits, sel, chunk_log2, c + hbm / SEG_BW};
+}
+
+// keys per sampler task: about 16 tasks per segment (load balance), 8K..128K
+// keys (ticket overhead), a whole number of subranges
+int tuned_chunk(uint32_t len, int alpha) {
+  const int c = (int)std::ceil(std::log2(std::max(1.0, len / 16.0)));
+  return std::max(alpha, std::max(13, std::min(c, 17)));
+}
+
+// The tuner: every field of `want` that is -1 is chosen; the others are
+// taken as given (checked).  Returns false for an impossible request.
+bool choose(uint32_t len, uint32_t k, int sorted, const drtopk_seg_params_t& want, double ctas, SegDesc& d) {
+  const int wa = want.algo, wal = want.alpha, wb = want.beta, wn = want.nbits, ws = want.bucket, wc = want.chunk_log2;
+  if (wn != -1 && wn != 4 && wn != 8) return false;
+  if (ws != -1 && ws != 0 && ws != 1) return false;
+  if (wb != -1 && wb != 1 && wb != 2) return false;
+  if (wc != -1 && (wc < 13 || wc > 20)) return false;
+  SegChoice best = {SEG_PLAIN, 0, 0, 8, SEG_RADIX, 0, 1e300};
+  auto consider = [&](const SegChoice& c) {
+    if (c.cost < best.cost) best = c;
+  };
+  for (int nbits : {8, 4}) {
+    if (wn != -1 && nbits != wn) continue;
+    for (int sel : {SEG_RADIX, SEG_BUCKET}) {
+      if (ws != -1 && sel != ws) continue;
+      if ((wa == -1 || wa == DRTOPK_ALGO_PLAIN_RADIX) && wal <= 0 && wb == -1 && wc == -1)
+        consider(cost_plain(len, k, sorted, nbits, sel, ctas));
+      if (wa == -1 || wa == DRTOPK_ALGO_RADIX) {
+        for (int alpha = 2; alpha <= 16; ++alpha) {
+          if (wal != -1 && alpha != wal) continue;
+          const uint64_t M = ((uint64_t)len + (1ull << alpha) - 1) >> alpha;
+          for (int beta : {1, 2}) {
+            if (wb != -1 && beta != wb) continue;
+            if (beta == 1 && M < k) continue;
+            if (beta == 2 && (2 * M < k || k > (uint32_t)SEG_B2_MAX_K)) continue;
+            const int ch = wc != -1 ? wc : tuned_chunk(len, alpha);
+            if (ch < alpha) continue;
+            consider(cost_delegate(len, k, sorted, alpha, beta, nbits, sel, ch, ctas));
+          }
+        }
+      }
+    }
   }
-  mode = SEG_DELEGATE;
-  alpha = a;
+  if ((wa == -1 || wa == DRTOPK_ALGO_BITONIC) && len <= (uint32_t)SEG_SORT_MAX && wal <= 0 && wb == -1 &&
+      (wn == -1 || wn == 8) && ws <= 0 && wc == -1)
+    consider(cost_bitonic(len, ctas));
+  if (best.cost >= 1e300) return false;
+  d.mode = best.mode;
+  d.alpha = best.alpha;
+  d.beta = best.mode == SEG_DELEGATE ? best.beta : 0;
+  d.nbits = best.nbits;
+  d.sel = best.sel;
+  d.chunk_log2 = best.mode == SEG_DELEGATE ? best.chunk_log2 : 0;
+  return true;
 }
 
 cudaError_t free_graph(drtopk_batch* b) {
@@ -136,8 +252,25 @@ extern "C" drtopk_status_t drtopk_batch_destroy(drtopk_batch_t b) {
 
 extern "C" drtopk_status_t drtopk_batch_plan(drtopk_batch_t b, int nseg, const uint64_t* h_offsets,
                                              const uint32_t* h_ks, const int* h_dtypes, int sorted) {
+  return drtopk_batch_plan_params(b, nseg, h_offsets, h_ks, h_dtypes, sorted, nullptr);
+}
+
+extern "C" drtopk_status_t drtopk_batch_plan_params(drtopk_batch_t b, int nseg, const uint64_t* h_offsets,
+                                                    const uint32_t* h_ks, const int* h_dtypes, int sorted,
+                                                    const drtopk_seg_params_t* h_params) {
   if (!b || nseg <= 0 || !h_offsets || !h_ks) return DRTOPK_EINVAL;
   std::lock_guard<std::mutex> lk(b->mu);
+  int grid = 0;
+  size_t smem = 0;
+  {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(b->device);
+    const cudaError_t e = segmented_shape(b->device, &grid, &smem);
+    cudaSetDevice(cur);
+    if (e != cudaSuccess) return DRTOPK_ECUDA;
+  }
+  const drtopk_seg_params_t tuned = {-1, -1, -1, -1, -1, -1};
   std::vector<SegDesc> seg(nseg);
   std::vector<uint2> tasks;
   uint64_t del_total = 0, cand_total = 0, out_total = 0;
@@ -155,16 +288,19 @@ extern "C" drtopk_status_t drtopk_batch_plan(drtopk_batch_t b, int nseg, const u
     d.k = k;
     d.sorted = sorted;
     d.km = dt == DRTOPK_F32 ? KM_F32 : KM_U32;
-    choose(d.len, k, d.mode, d.alpha);
+    if (!choose(d.len, k, sorted, h_params ? h_params[s] : tuned, (double)grid, d)) return DRTOPK_EINVAL;
     d.out_off = out_total;
     out_total += k;
     if (d.mode == SEG_DELEGATE) {
       const uint64_t S = 1ull << d.alpha, M = (len + S - 1) >> d.alpha;
       d.del_off = del_total;
-      del_total += M;
+      del_total += M * (d.beta == 2 ? 3 : 1);
       d.cand_off = cand_total;
-      cand_total += (uint64_t)k * S;
-      d.ntasks = (int)((len + SEG_CH - 1) / SEG_CH);
+      // beta 1: the k kept subranges; beta 2: fewer than 2k read whole and
+      // fewer than k single Maxes
+      cand_total += d.beta == 2 ? 2 * (uint64_t)k * S + k : (uint64_t)k * S;
+      const uint64_t CH = 1ull << d.chunk_log2;
+      d.ntasks = (int)((len + CH - 1) / CH);
       for (int c = 0; c < d.ntasks; ++c) tasks.push_back(make_uint2((uint32_t)s, (uint32_t)c));
     } else {
       d.ntasks = 0;
@@ -287,13 +423,27 @@ extern "C" drtopk_status_t drtopk_batch_sync_check(drtopk_batch_t b, void* strea
   return s;
 }
 
+static int seg_algo(const SegDesc& d) {
+  return d.mode == SEG_DELEGATE ? DRTOPK_ALGO_RADIX
+                                : (d.mode == SEG_BITONIC ? DRTOPK_ALGO_BITONIC : DRTOPK_ALGO_PLAIN_RADIX);
+}
+
 extern "C" drtopk_status_t drtopk_batch_describe(drtopk_batch_t b, int* h_algo, int* h_alpha, int* h_beta) {
   if (!b || b->nseg == 0) return DRTOPK_EINVAL;
   for (int s = 0; s < b->nseg; ++s) {
     const SegDesc& d = b->seg[s];
-    if (h_algo) h_algo[s] = d.mode == SEG_DELEGATE ? DRTOPK_ALGO_RADIX : DRTOPK_ALGO_PLAIN_RADIX;
+    if (h_algo) h_algo[s] = seg_algo(d);
     if (h_alpha) h_alpha[s] = d.alpha;
-    if (h_beta) h_beta[s] = d.mode == SEG_DELEGATE ? 1 : 0;
+    if (h_beta) h_beta[s] = d.beta;
+  }
+  return DRTOPK_OK;
+}
+
+extern "C" drtopk_status_t drtopk_batch_describe_params(drtopk_batch_t b, drtopk_seg_params_t* h_params) {
+  if (!b || b->nseg == 0 || !h_params) return DRTOPK_EINVAL;
+  for (int s = 0; s < b->nseg; ++s) {
+    const SegDesc& d = b->seg[s];
+    h_params[s] = {seg_algo(d), d.alpha, d.beta, d.nbits, d.sel, d.chunk_log2};
   }
   return DRTOPK_OK;
 }

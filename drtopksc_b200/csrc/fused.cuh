@@ -343,21 +343,25 @@ DRTOPK_DEV uint64_t* grid_lsd_sort(const Team& tm, const FusedArgs& a, uint64_t*
   const int C = (int)tm.size, c = (int)tm.rank, t = threadIdx.x;
   const uint32_t per = (nk + C - 1) / C;
   const uint32_t r0 = min(nk, per * c), r1 = min(nk, r0 + per);
-  // totals of all 8 digits
-  for (int d = 0; d < 8; ++d) {
-    for (int i = t; i < 256; i += blockDim.x) s_cnt[i] = 0;
-    __syncthreads();
-    block_load_loop<8>(r1 - r0, [&](uint32_t i) { return ld_cg_u64(src + r0 + i); },
-                       [&](uint32_t, uint64_t v) { atomicAdd(&s_cnt[(v >> (8 * d)) & 255u], 1u); });
-    __syncthreads();
-    for (int i = t; i < 256; i += blockDim.x)
-      if (s_cnt[i]) atomicAdd(&a.sort_tot[d * 256 + i], s_cnt[i]);
-    __syncthreads();
-  }
-  if (!team_sync(tm)) { ok = false; return src; }
   __shared__ uint32_t s_run[256];
   __shared__ uint32_t s_wcnt[MAX_BLOCK_WARPS][257];
   __shared__ int s_trivial;
+  // totals of all 8 digits, in one pass over this CTA's range (8 x 256
+  // counters in the scatter's per-warp count space, unused until then)
+  uint32_t* s_tot8 = &s_wcnt[0][0];
+  for (int i = t; i < 8 * 256; i += blockDim.x) s_tot8[i] = 0;
+  __syncthreads();
+  block_load_loop<8>(r1 - r0, [&](uint32_t i) { return ld_cg_u64(src + r0 + i); }, [&](uint32_t, uint64_t v) {
+#pragma unroll
+    for (int d = 0; d < 8; ++d) atomicAdd(&s_tot8[d * 256 + ((v >> (8 * d)) & 255u)], 1u);
+  });
+  __syncthreads();
+  for (int i = t; i < 8 * 256; i += blockDim.x) {
+    const uint32_t c = s_tot8[i];
+    if (c) atomicAdd(&a.sort_tot[i], c);
+  }
+  __syncthreads();
+  if (!team_sync(tm)) { ok = false; return src; }
   for (int d = 0; d < 8; ++d) {
     if (t == 0) s_trivial = 0;
     __syncthreads();

@@ -292,8 +292,31 @@ DRTOPK_API drtopk_status_t drtopk_batch_run(drtopk_batch_t b, const void* d_keys
 DRTOPK_API drtopk_status_t drtopk_batch_run_graph(drtopk_batch_t b, const void* d_keys, void* d_kth, void* d_vals,
                                        int64_t* d_idx, void* stream);
 DRTOPK_API drtopk_status_t drtopk_batch_sync_check(drtopk_batch_t b, void* stream);
-/* Per-segment choice of the autotuner: h_algo[nseg], h_alpha[nseg] (host). */
+/* Per-segment choice of the autotuner: h_algo[nseg], h_alpha[nseg], h_beta[nseg] (host). */
 DRTOPK_API drtopk_status_t drtopk_batch_describe(drtopk_batch_t b, int* h_algo, int* h_alpha, int* h_beta);
+
+/* Per-segment knobs of the batched form (the reference sets them per run:
+ * alphaManualTuning/main.cu:83-84, bucket_select/main.cu:57-67,
+ * bitonic/sampleBitonic.cu:194-204).  drtopk_batch_plan_params takes one per
+ * segment (host array; NULL = all tuned) with -1 in any field the autotuner
+ * should pick; drtopk_batch_describe_params returns the choice.
+ *   algo        DRTOPK_ALGO_PLAIN_RADIX (block select over the raw keys),
+ *               DRTOPK_ALGO_RADIX (delegates, then the block selects),
+ *               DRTOPK_ALGO_BITONIC (every key sorted in shared memory;
+ *               segments of <= 4096 keys)
+ *   alpha       log2 subrange size (delegate segments; 0 otherwise)
+ *   beta        delegates per subrange: 1 (Max) or 2 (Max, Second; k <= 1365)
+ *   nbits       digit width of the block selects: 4 or 8 (2^nbits bins)
+ *   bucket      0: radix digits; 1: min/max buckets (the reference's bucket
+ *               select, exact) in the block selects
+ *   chunk_log2  keys per sampler task, 2^chunk_log2 (13..20, >= alpha) */
+typedef struct {
+  int algo, alpha, beta, nbits, bucket, chunk_log2;
+} drtopk_seg_params_t;
+DRTOPK_API drtopk_status_t drtopk_batch_plan_params(drtopk_batch_t b, int nseg, const uint64_t* h_offsets,
+                                                    const uint32_t* h_ks, const int* h_dtypes, int sorted,
+                                                    const drtopk_seg_params_t* h_params);
+DRTOPK_API drtopk_status_t drtopk_batch_describe_params(drtopk_batch_t b, drtopk_seg_params_t* h_params);
 
 /* ---------------------------------------------------------------------
  * Served form: continuous batching of top-k requests under an HBM budget.

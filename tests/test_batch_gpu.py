@@ -67,8 +67,61 @@ def test_batch_matches_oracle(sorted):
     segs, bits, offsets, ks, dtypes = make_batch(1, 60, 10, 20)
     b, kth, vals, idx = run_batch(bits, offsets, ks, dtypes, sorted=sorted)
     algo, alpha, beta = b.describe()
-    assert (algo == 0).any() and (algo == 3).any()  # both delegate and plain segments present
+    assert (algo == 0).any()  # delegate segments present (short ones: plain or bitonic)
+    kn = b.describe_params()
+    assert all(q["nbits"] in (4, 8) and q["bucket"] in (0, 1) for q in kn)
+    assert all(q["chunk_log2"] >= q["alpha"] for q in kn if q["algo"] == 0)
     check_segments(segs, ks, b, kth, vals, idx, sorted)
+
+
+# every knob of drtopk_seg_params_t, forced per segment
+KNOBS = ([{"algo": "plain", "nbits": nb, "bucket": bk} for nb in (4, 8) for bk in (0, 1)] +
+         [{"algo": "radix", "alpha": al, "beta": be, "nbits": nb, "bucket": bk, "chunk_log2": ch}
+          for al, ch in ((6, 13), (9, 15), (12, 17)) for be in (1, 2) for nb in (4, 8) for bk in (0, 1)] +
+         [{"algo": "bitonic"}])
+
+
+@pytest.mark.parametrize("sorted", [True, False])
+def test_batch_every_forced_knob_matches_oracle(sorted):
+    import torch
+
+    import drtopksc_b200 as D
+    rng = np.random.default_rng(7)
+    segs, ks, params = [], [], []
+    for i, q in enumerate(KNOBS):
+        for dist in ("u32", "f32n", "fewdigits", "ties"):
+            n = int(rng.integers(1500, 4096)) if q["algo"] == "bitonic" else int(rng.integers(40000, 300000))
+            if dist == "ties":
+                x = np.repeat(rng.integers(0, 40, (n + 999) // 1000).astype(np.uint32), 1000)[:n].copy()
+            else:
+                x = O.gen(dist, n, 100 * i + len(segs))
+            kmax = 1365 if q.get("beta") == 2 else 4096
+            k = int(min(n, kmax, np.exp2(rng.uniform(0, 12))))
+            if q["algo"] == "radix":  # the delegate vector must hold k
+                k = min(k, (n >> q["alpha"]) * q["beta"])
+            segs.append(x)
+            ks.append(max(1, k))
+            params.append(q)
+    ks = np.array(ks, dtype=np.uint32)
+    bits = np.concatenate([x.view(np.uint32) for x in segs])
+    offsets = np.concatenate([[0], np.cumsum([x.size for x in segs])]).astype(np.uint64)
+    dtypes = np.array([1 if x.dtype == np.float32 else 0 for x in segs], dtype=np.int32)
+    b = D.Batch().plan(offsets, ks, dtypes, sorted=sorted, params=params)
+    got = b.describe_params()
+    for q, g in zip(params, got):
+        for f, v in q.items():
+            if f == "algo":
+                v = D._ALGOS[v]
+            assert g[f] == v, (q, g)
+    keys = torch.from_numpy(bits.view(np.int32)).cuda()
+    kth = torch.zeros(len(ks), dtype=torch.int32, device="cuda")
+    tot = int(ks.astype(np.int64).sum())
+    vals = torch.zeros(tot, dtype=torch.int32, device="cuda")
+    idx = torch.zeros(tot, dtype=torch.int64, device="cuda")
+    b.run(keys, kth, vals, idx)
+    b.sync_check()
+    check_segments(segs, ks, b, kth.cpu().numpy().view(np.uint32), vals.cpu().numpy().view(np.uint32),
+                   idx.cpu().numpy(), sorted)
 
 
 def test_batch_graph_replay_and_heavy_ties():
@@ -98,6 +151,12 @@ def test_batch_equals_plain_calls():
 def test_batch_argument_errors():
     import drtopksc_b200 as D
     b = D.Batch()
+    with pytest.raises(D.DrTopKError) as e:  # bitonic segments hold at most 4096 keys
+        b.plan([0, 10000], [5], [0], params=[{"algo": "bitonic"}])
+    assert e.value.status == D.EINVAL
+    with pytest.raises(D.DrTopKError) as e:  # beta 2 keeps up to 3k subranges: k <= 1365
+        b.plan([0, 1 << 20], [2000], [0], params=[{"algo": "radix", "beta": 2}])
+    assert e.value.status == D.EINVAL
     with pytest.raises(D.DrTopKError) as e:
         b.plan([0, 10], [11], [0])
     assert e.value.status == D.EINVAL
