@@ -66,22 +66,22 @@ inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 // off on keys of a narrow range, which a caller can ask for) and 4-bit
 // digits as twice the passes.
 // Calibrated on B200 against forced-knob runs of the 4096-segment batch
-// (lengths 2^10..2^22): a block pass is latency-bound (~2K entries per us and
-// a few us of barriers and picks); a delegate entry costs about five times a
-// candidate entry (the alpha that minimised the batch time sits at
-// 2^alpha ~ sqrt(5 len / k)) and a raw key of a plain segment about 2.5
-// (plain segments were fastest up to ~16K keys); the bitonic network of a whole segment loses
-// to the radix passes from ~1K keys up; and the beta-2 sampler's top-two
-// bookkeeping costs about as much as the keys' HBM time.
+// (lengths 2^10..2^22): a block pass is latency-bound (~2K entries per us
+// and a few us of barriers and picks); a delegate entry costs about six
+// times a candidate entry (the fastest alpha sat near 2^alpha ~
+// sqrt(5 len / k)) and a raw key of a plain segment about 2.5 (plain
+// segments were fastest up to ~16K keys); the bitonic network of a whole
+// segment lost to the radix passes from ~1K keys up; and the beta-2
+// sampler's top-two bookkeeping costs about as much as the keys' HBM time.
 constexpr double SEG_BW = 6.0e6;        // HBM bytes per us (whole GPU)
 constexpr double SEG_T_PASS = 4.0;      // us per block pass (one CTA)
 constexpr double SEG_T_ELEM = 0.0005;   // us per entry per pass (one CTA)
-constexpr double SEG_DEL_WEIGHT = 5.0;  // a delegate entry against a candidate entry
+constexpr double SEG_DEL_WEIGHT = 6.0;  // a delegate entry against a candidate entry
 constexpr double SEG_KEY_WEIGHT = 2.5;  // a raw key of a plain segment against a candidate entry
 constexpr double SEG_T_TASK = 1.0;      // us per sampler task (ticket, barriers)
 constexpr double SEG_T_SAMP = 0.0006;   // us per key sampled (one CTA)
 constexpr double SEG_T_SAMP2 = 8.6e-7;  // us of batch time per key: beta 2's top-two sampler
-constexpr double SEG_T_STAGE = 0.6;     // us per bitonic stage (one CTA, up to 4096 entries)
+constexpr double SEG_T_STAGE = 1.0;     // us per bitonic stage (one CTA, up to 4096 entries)
 
 struct SegChoice {
   int mode, alpha, beta, nbits, sel, chunk_log2;
