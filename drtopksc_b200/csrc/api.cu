@@ -429,7 +429,7 @@ void layout(Plan* P, bool want_idx) {
   // always uses 8-bit digits even when the bucket variant has fewer buckets
   P->hist_words = std::max(P->nb, 256);
   P->run_words = 3 * P->hist_words + (MAX_LEVELS + 2) + 1 + 4;
-  size_t ctrl_words = CTRL_HDR_WORDS + 4 * (size_t)P->run_words + 8 * 256;
+  size_t ctrl_words = CTRL_HDR_WORDS + 4 * (size_t)P->run_words + 8 * 256 + 8;  // large-k sort: totals + flag
   P->pre_hist_word = ctrl_words;
   ctrl_words += PRE_STATE + PRE_STATE_WORDS;  // sampled-threshold path: one 256-bin histogram per byte level
                                                // of the key sample, then the walk's state

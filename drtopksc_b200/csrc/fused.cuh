@@ -32,6 +32,9 @@ namespace drtopk {
 enum Path : int { PATH_DEFAULT = 0, PATH_BETA = 1, PATH_PLAIN = 2, PATH_BITONIC = 3, PATH_EMIT = 4 };
 
 constexpr int SMALL_SORT = 4096;  // top-k sorted in one CTA's shared memory up to this k
+constexpr int TIE_RUN_MAX = 32;   // large-k sort: longest run of equal keys put in index order by one thread
+constexpr int SORT_U = 4;         // large-k sort: keys per thread per scatter round
+constexpr int SORT_LONG_WORD = 8 * 256;  // sort_tot word after the digit totals: a longer run was found
 
 struct FusedArgs {
   const uint32_t* keys;
@@ -63,7 +66,7 @@ struct FusedArgs {
   int sorted;
   uint64_t* sort_buf[2];  // [k] each (large sorted output)
   uint32_t* sort_cnt;     // [grid][256]
-  uint32_t* sort_tot;     // [8][256]
+  uint32_t* sort_tot;     // [8][256] digit totals, then the long-run flag
   uint32_t* stats;        // [16]
   uint32_t* thr_word;     // threshold handed between launches in split mode
   uint32_t* tail_flag;    // shared-memory tail: 1 done, 2 fall back to the general path
@@ -357,18 +360,20 @@ DRTOPK_DEV uint64_t* grid_lsd_sort(const Team& tm, const FusedArgs& a, uint64_t*
   });
   __syncthreads();
   for (int i = t; i < 8 * 256; i += blockDim.x) {
-    const uint32_t c = s_tot8[i];
-    if (c) atomicAdd(&a.sort_tot[i], c);
+    const uint32_t cnt = s_tot8[i];
+    if (cnt) atomicAdd(&a.sort_tot[i], cnt);
   }
   __syncthreads();
   if (!team_sync(tm)) { ok = false; return src; }
-  for (int d = 0; d < 8; ++d) {
+  // one stable counting pass over digit d (src -> dst, then swapped); a
+  // digit every key shares is skipped
+  auto digit_pass = [&](int d) -> bool {
     if (t == 0) s_trivial = 0;
     __syncthreads();
     for (int i = t; i < 256; i += blockDim.x)
       if (ld_cg_u32(a.sort_tot + d * 256 + i) == nk) s_trivial = 1;
     __syncthreads();
-    if (s_trivial) continue;
+    if (s_trivial) return true;
     const int sh = 8 * d;
     // 1) this CTA's digit counts
     for (int i = t; i < 256; i += blockDim.x) s_cnt[i] = 0;
@@ -377,7 +382,7 @@ DRTOPK_DEV uint64_t* grid_lsd_sort(const Team& tm, const FusedArgs& a, uint64_t*
                        [&](uint32_t, uint64_t v) { atomicAdd(&s_cnt[(v >> sh) & 255u], 1u); });
     __syncthreads();
     for (int i = t; i < 256; i += blockDim.x) a.sort_cnt[(uint64_t)c * 256 + i] = s_cnt[i];
-    if (!team_sync(tm)) { ok = false; return src; }
+    if (!team_sync(tm)) return false;
     // 2) exclusive scan of each digit column over the CTAs (in place)
     for (int col = c; col < 256; col += C) {
       if (t < 32) {
@@ -396,7 +401,7 @@ DRTOPK_DEV uint64_t* grid_lsd_sort(const Team& tm, const FusedArgs& a, uint64_t*
         }
       }
     }
-    if (!team_sync(tm)) { ok = false; return src; }
+    if (!team_sync(tm)) return false;
     // 3) running offsets = digit base (scan of totals) + this CTA's column prefix
     if (t < 256) s_cnt[t] = ld_cg_u32(a.sort_tot + d * 256 + t);
     __syncthreads();
@@ -407,36 +412,94 @@ DRTOPK_DEV uint64_t* grid_lsd_sort(const Team& tm, const FusedArgs& a, uint64_t*
     __syncthreads();
     if (t < 256) s_run[t] = s_cnt[t] + ld_cg_u32(a.sort_cnt + (uint64_t)c * 256 + t);
     __syncthreads();
-    // 4) stable scatter in chunks of blockDim keys
+    // 4) stable scatter in chunks of SORT_U keys per thread: warp w takes
+    // the chunk's w-th span of 32 * SORT_U keys, in SORT_U rounds of 32
+    // consecutive ones, so its ranks follow position order; the warps'
+    // counts then give each warp its prefix per digit
     const int wid = t >> 5;
+    const int nwarps = (int)(blockDim.x >> 5);
     const unsigned lane = t & 31u;
-    for (uint32_t cb = r0; cb < r1; cb += blockDim.x) {
-      const uint32_t i = cb + t;
-      const bool valid = i < r1;
-      const uint64_t key = valid ? ld_cg_u64(src + i) : 0ull;
-      const uint32_t dg = valid ? (uint32_t)((key >> sh) & 255u) : 256u;
+    const uint32_t CHK = blockDim.x * SORT_U;
+    for (uint32_t cb = r0; cb < r1; cb += CHK) {
       for (int q = lane; q < 257; q += 32) s_wcnt[wid][q] = 0;
       __syncwarp();
-      const unsigned peers = __match_any_sync(0xffffffffu, dg);
-      const uint32_t rank_in_warp = __popc(peers & ((1u << lane) - 1u));
-      if (rank_in_warp == 0) s_wcnt[wid][dg] = __popc(peers);
-      __syncthreads();
-      if (valid) {
-        uint32_t before_w = 0;
-        for (int w2 = 0; w2 < wid; ++w2) before_w += s_wcnt[w2][dg];
-        dst[s_run[dg] + before_w + rank_in_warp] = key;
+      uint64_t kv[SORT_U];
+      uint32_t dgs[SORT_U], rk[SORT_U];
+      const uint32_t wb = cb + (uint32_t)wid * 32u * SORT_U;
+#pragma unroll
+      for (int u = 0; u < SORT_U; ++u) {
+        const uint32_t i = wb + (uint32_t)u * 32u + lane;
+        kv[u] = i < r1 ? ld_cg_u64(src + i) : 0ull;
+      }
+#pragma unroll
+      for (int u = 0; u < SORT_U; ++u) {
+        const uint32_t i = wb + (uint32_t)u * 32u + lane;
+        const uint32_t dg = i < r1 ? (uint32_t)((kv[u] >> sh) & 255u) : 256u;
+        const unsigned peers = __match_any_sync(0xffffffffu, dg);
+        const uint32_t lower = __popc(peers & ((1u << lane) - 1u));
+        rk[u] = s_wcnt[wid][dg] + lower;
+        dgs[u] = dg;
+        __syncwarp();
+        if (lower == 0) s_wcnt[wid][dg] += __popc(peers);
+        __syncwarp();
       }
       __syncthreads();
-      for (int q = t; q < 256; q += blockDim.x) {
-        uint32_t add = 0;
-        for (int w2 = 0; w2 < (int)(blockDim.x / 32); ++w2) add += s_wcnt[w2][q];
-        s_run[q] += add;
+      // per digit: the warps' counts become their exclusive prefixes
+      uint32_t dtot = 0;
+      if (t < 256) {
+        for (int w2 = 0; w2 < nwarps; ++w2) {
+          const uint32_t v = s_wcnt[w2][t];
+          s_wcnt[w2][t] = dtot;
+          dtot += v;
+        }
       }
       __syncthreads();
+#pragma unroll
+      for (int u = 0; u < SORT_U; ++u)
+        if (dgs[u] < 256u) dst[s_run[dgs[u]] + s_wcnt[wid][dgs[u]] + rk[u]] = kv[u];
+      __syncthreads();
+      if (t < 256) s_run[t] += dtot;
     }
-    if (!team_sync(tm)) { ok = false; return src; }
+    if (!team_sync(tm)) return false;
     uint64_t* tmp = src; src = dst; dst = tmp;
+    return true;
+  };
+  // The key's digits first (4..7): the passes are stable, so equal keys
+  // keep their input order; then every run of equal keys is put in index
+  // order in place, one thread per run.  Runs longer than TIE_RUN_MAX (heavy
+  // ties) set a flag, and the keys then go through all eight digits from
+  // the least significant, the plain LSD order.
+  for (int d = 4; d < 8; ++d)
+    if (!digit_pass(d)) { ok = false; return src; }
+  __shared__ int s_long;
+  if (t == 0) s_long = 0;
+  __syncthreads();
+  const uint64_t g = (uint64_t)c * blockDim.x + t, G = (uint64_t)C * blockDim.x;
+  for (uint64_t i = g; i < nk; i += G) {
+    const uint32_t hk = (uint32_t)(ld_cg_u64(src + i) >> 32);
+    if (i > 0 && (uint32_t)(ld_cg_u64(src + i - 1) >> 32) == hk) continue;  // not a run start
+    uint64_t e = i + 1;
+    while (e < nk && e - i <= (uint64_t)TIE_RUN_MAX && (uint32_t)(ld_cg_u64(src + e) >> 32) == hk) ++e;
+    if (e - i > (uint64_t)TIE_RUN_MAX) { s_long = 1; continue; }
+    // insertion sort of the run by index, in a thread-local copy (the run's
+    // loads are independent; the sort's compares are not)
+    uint64_t run[TIE_RUN_MAX];
+    const int m = (int)(e - i);
+    for (int x = 0; x < m; ++x) run[x] = ld_cg_u64(src + i + x);
+    for (int x = 1; x < m; ++x) {
+      const uint64_t v = run[x];
+      int y = x;
+      for (; y > 0 && run[y - 1] > v; --y) run[y] = run[y - 1];
+      run[y] = v;
+    }
+    for (int x = 0; x < m; ++x) src[i + x] = run[x];
   }
+  __syncthreads();
+  if (t == 0 && s_long) atomicOr(a.sort_tot + SORT_LONG_WORD, 1u);
+  if (!team_sync(tm)) { ok = false; return src; }
+  if (ld_cg_u32(a.sort_tot + SORT_LONG_WORD))
+    for (int d = 0; d < 8; ++d)
+      if (!digit_pass(d)) { ok = false; return src; }
   return src;
 }
 

@@ -160,6 +160,20 @@ def test_large_sorted_k_uses_grid_sort():
     check_exact(f, 70000)
 
 
+@pytest.mark.parametrize("copies", [2, 9, 32, 33, 3000])
+def test_large_sorted_k_runs_of_equal_keys(copies):
+    # the large-k sort orders the keys first, then each run of equal keys by
+    # index; runs longer than 32 send it through every digit instead
+    rng = np.random.default_rng(copies)
+    n = 1 << 19
+    vals = rng.integers(0, 1 << 32, size=n // copies + 1, dtype=np.uint64).astype(np.uint32)
+    x = np.repeat(vals, copies)[:n]
+    rng.shuffle(x)
+    for k in (5000, 1 << 17):
+        check_exact(x, k)
+        check_exact(x, k, alpha=-2)
+
+
 def test_heavy_ties():
     for x in (np.full(1 << 16, 7, dtype=np.uint32), np.zeros(5000, dtype=np.uint32),
               np.full(4096, 0xFFFFFFFF, dtype=np.uint32),
