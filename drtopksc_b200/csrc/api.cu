@@ -1519,15 +1519,14 @@ extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_
     }
   }
   // the sampled-threshold path (path 4): one streaming pass that appends
-  // every key at or above a threshold predicted from a 1/64 key sample;
+  // every key at or above a threshold predicted from a strided key sample;
   // calibrated on B200: the pass streams at ~1.1 of the copy bandwidth,
-  // ~50 us fixed (two sample passes, five launches, the last levels), and
+  // ~50 us fixed (the sample passes, seven launches, the last levels), and
   // ~73 bytes' worth per candidate (append, level-0 split, last levels).
   // Candidates: k plus the six-sigma margin plus one 16-bit prefix bin.
   bool best_emit = false;
   if (p->algo == DRTOPK_ALGO_RADIX && n >= (1ull << 20)) {
-    const double ks = dk / 64.0;
-    const double cand = dk + 64.0 * (6.0 * std::sqrt(ks) + 16.0) + dn / 65536.0;
+    const double cand = emit_cand_estimate(n, k, pre_stride_for(n));
     const double c = 4.0 * dn / 1.1 + 50.0 * TAIL_BYTES_PER_US + 73.0 * cand;
     // float keys crowd into few exponent bins: the delegate paths' fixed
     // threshold digits can then admit a large share of the keys (uniform
