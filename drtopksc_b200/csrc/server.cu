@@ -601,9 +601,13 @@ void drtopk_server::prewarm() {
   cudaStreamSynchronize(st);
   static std::once_flag once;
   std::call_once(once, [this]() {
+    // pinned staging of every size class a chain's results can need, more
+    // copies of the small classes (at light load many small chains are in
+    // flight at once); a miss on the serving path costs a cudaHostAlloc of
+    // milliseconds
     std::vector<std::pair<void*, size_t>> got;
-    for (size_t c = size_t(1) << 20; c <= 4 * GROUP_OUT_CAP; c <<= 1)
-      for (int i = 0; i < 2; ++i) {
+    for (size_t c = size_t(64) << 10; c <= 4 * GROUP_OUT_CAP; c <<= 1)
+      for (int i = 0, copies = c <= (size_t(4) << 20) ? 8 : (c <= GROUP_OUT_CAP ? 4 : 2); i < copies; ++i) {
         size_t cap = 0;
         void* b = pinned.get(c, &cap);
         if (b) got.emplace_back(b, cap);
