@@ -1476,6 +1476,47 @@ static double tail_beta(double n, double k, double S, int digits) {
   return 2.8 * cost_beta(n, k, S, digits) + 20.0 * TAIL_BYTES_PER_US;
 }
 
+// Small k is latency, not bytes.  When the delegates, the kept subranges and
+// the candidates fit one CTA's shared memory, the phases after the sampler run
+// in one CTA (the tail eligibility rule of plan_for, mirrored here); its chain
+// of dependent levels costs ~1.8 us per 1K delegates plus ~0.33 us per 1K
+// gathered keys on the one-delegate path, ~2 us per 1K delegate values plus
+// ~0.08 us per wanted key on the beta path, where the multi-CTA phases that
+// the tail terms above were calibrated on cost ~40 us (measured on B200 at
+// n = 2^16..2^22, k = 1..128, where the bandwidth terms are flat).  Returned
+// as a correction to those terms, in bytes at the HBM roofline; 0 for k above
+// SMALL_K_TUNE, where the bandwidth model alone was measured to choose well.
+constexpr uint64_t SMALL_K_TUNE = 256;
+static double small_k_latency(double n, double k, double S, int path, int digits, const drtopk_params_t* p) {
+  if (k > (double)SMALL_K_TUNE) return 0.0;
+  const double M = std::ceil(n / S), Md = path == 1 ? M : 2.0 * M;
+  bool fits = p->algo == DRTOPK_ALGO_RADIX && p->nbits <= 8 && Md <= (double)TAIL_CAP &&
+              k <= (double)TAIL_CAP && (!p->sorted || k <= (double)SMALL_SORT);
+  double gather = 0.0, cand = 0.0;
+  if (path == 1) {
+    gather = k * S;
+    cand = k;
+  } else {
+    const double q = k / n + std::ldexp(1.0, -8 * std::max(1, digits));
+    const double lam = q * S, e = std::exp(-lam), Mf = n / S;
+    const double p_sel = 1.0 - e * (1.0 + lam);
+    gather = Mf * p_sel * S;
+    cand = Mf * lam * e + Mf * p_sel * (lam + 1.0);
+  }
+  fits = fits && gather <= TAIL_GATHER_AUTO && cand <= TAIL_CAP / 2;
+  if (!fits) return 0.0;
+  const double us = path == 1 ? 1.8 * M / 1024.0 + 0.33 * gather / 1024.0 : 2.0 * Md / 1024.0 + 0.08 * k;
+  return (us - 40.0) * TAIL_BYTES_PER_US;
+}
+
+// The sampler's pass: all keys at the sampler's measured share of the copy
+// bandwidth, but no faster than one warp streams its own subrange (~4 GB/s
+// per warp), which binds when few large subranges cover a small input.
+static double sampler_bytes(double n, int alpha, bool beta2, bool f32, double M) {
+  const double floor_us = std::ldexp(4.0, alpha) / 4000.0;
+  return std::max(4.0 * n / sampler_eff(alpha, beta2, f32, M), floor_us * TAIL_BYTES_PER_US);
+}
+
 extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_t dtype, drtopk_params_t* p) {
   if (!p || n == 0 || k < 1 || k > n) return DRTOPK_EINVAL;
   if (p->algo == DRTOPK_ALGO_AUTO) p->algo = DRTOPK_ALGO_RADIX;
@@ -1488,8 +1529,10 @@ extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_
     }
     return DRTOPK_OK;
   }
-  // small inputs: the delegate pass does not pay for itself
-  if (n <= (1ull << 16) && p->algo == DRTOPK_ALGO_RADIX) {
+  // small inputs: the delegate pass does not pay for itself (for k <= 64 it
+  // does from 2^13 keys, where the plain select no longer fits one CTA:
+  // 29 us against 36-40 us at n = 2^14..2^16 on B200)
+  if (n <= (1ull << 16) && p->algo == DRTOPK_ALGO_RADIX && (n <= (uint64_t)TAIL_CAP || k > 64)) {
     p->algo = DRTOPK_ALGO_PLAIN_RADIX;
     p->alpha = 0;
     return DRTOPK_OK;
@@ -1503,7 +1546,8 @@ extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_
     const bool f32 = dtype == DRTOPK_F32;
     if (alpha >= 2 && M >= k) {
       // the sampler's pass over the keys (at its measured speed) plus the tail
-      const double c = 4.0 * dn / sampler_eff(alpha, false, f32, (double)M) + tail_default(dn, dk, S);
+      const double c = sampler_bytes(dn, alpha, false, f32, (double)M) + tail_default(dn, dk, S) +
+                       small_k_latency(dn, dk, S, 1, 0, p);
       if (c < best) { best = c; best_alpha = alpha; best_path = 1; best_digits = 0; }
     }
     if (2 * M >= k && p->beta == 2) {
@@ -1512,8 +1556,9 @@ extern "C" drtopk_status_t drtopk_autotune(uint64_t n, uint64_t k, drtopk_dtype_
       const int maxd = p->nbits == 8 ? 2 : 1;
       const int mind = (p->nbits == 8 && dtype == DRTOPK_F32) ? 2 : 1;
       for (int d = mind; d <= maxd; ++d) {
-        const double c = 4.0 * dn / sampler_eff(alpha, true, f32, (double)M) +
-                         tail_beta(dn, dk, S, p->nbits == 8 ? d : (32 / p->nbits - 3));
+        const int digits = p->nbits == 8 ? d : (32 / p->nbits - 3);
+        const double c = sampler_bytes(dn, alpha, true, f32, (double)M) + tail_beta(dn, dk, S, digits) +
+                         small_k_latency(dn, dk, S, 2, digits, p);
         if (c < best) { best = c; best_alpha = alpha; best_path = 2; best_digits = d; }
       }
     }
