@@ -523,17 +523,24 @@ void drtopk_server::launch_group(std::vector<Req*>& v, int si) {
   if (ok && enqueue_group(device, v[0]->plan.km, items.data(), np, hst + out_total, arena + o_desc,
                          reinterpret_cast<uint32_t*>(arena + out0 + o_err), st) != DRTOPK_OK)
     ok = false;
-  if (ok && cudaMemcpyAsync(hst, arena + out0, out_total, cudaMemcpyDeviceToHost, st) != cudaSuccess) ok = false;
-  if (arena) cudaFreeAsync(arena, st);
+  // the outputs' copy back and the arena's release on the compute stream's
+  // own copy stream: the next chain's kernels do not queue behind the
+  // device-to-host engine
+  const int xsi = ST_COPY + si;
+  cudaStream_t xs = streams[xsi];
+  cudaEventRecord(ev_kernels, st);
+  cudaStreamWaitEvent(xs, ev_kernels, 0);
+  if (ok && cudaMemcpyAsync(hst, arena + out0, out_total, cudaMemcpyDeviceToHost, xs) != cudaSuccess) ok = false;
+  if (arena) cudaFreeAsync(arena, xs);
   for (int i = 0; i < np; ++i) {
     Req* r = v[i];
     r->stream = si;
-    r->ev_stream = si;
+    r->ev_stream = xsi;
     r->hout = hst ? hst + o_out[i] : nullptr;
     r->hout_cap = 0;  // a view into the group's staging (owned by the last request)
     r->errp = hst ? reinterpret_cast<const uint32_t*>(hst + o_err) + i : nullptr;
     if (!ok) r->status = DRTOPK_ECUDA;
-    cudaEventRecord(r->ev, st);
+    cudaEventRecord(r->ev, xs);
   }
   // the staging is released with the last request (its completion event is
   // recorded after the copy)
