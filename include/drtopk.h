@@ -69,7 +69,7 @@ typedef struct {
   int sorted;       /* 1: top-k sorted by key (best first), ties by index ascending */
   int first_digits; /* beta path: digits used by the first select; 0: reference (32/nbits-3);
                        > 0: exactly this many; < 0 (the autotuner's choice): at least -first_digits,
-                       refined while the chosen bin still holds more than max(2k, 4096) delegates */
+                       refined while the chosen bin still holds more than max(2k, 256) delegates */
   int team;         /* CTAs running the phases after the sampler: 0 auto, 1 the whole GPU
                        (cooperative grid), 2 one thread-block cluster, 3 one CTA with the sets
                        in shared memory (small problems), 4 shared GPU: as auto, but a
