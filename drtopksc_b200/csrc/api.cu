@@ -616,8 +616,15 @@ static drtopk_status_t plan_for(int device, uint64_t n, uint64_t k, drtopk_dtype
         (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)di->sms * PRE_CTAS_PER_SM, nsw));
     const uint64_t nct = ((n + 511) / 512 + SPLIT_WARPS - 1) / SPLIT_WARPS;
     P->emit_grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)P->emit_grid, nct));
-    // team 5: every launch an ordinary one, the last levels in one CTA
-    P->one_cta = (p && p->team == 5 && fused_one_ready(di->device, P->km, smem)) ? 1 : 0;
+    // team 5: every launch an ordinary one, the last levels in one CTA.  The
+    // automatic team takes it too for unsorted outputs with k <= n/2048: the
+    // bin left after level 0 is then small, and one CTA finishes it sooner
+    // than the cooperative kernel's grid barriers (measured on B200 over the
+    // n = 2^30 sweep: 1-2 % faster at k = 2^17..2^19, even at 2^20, slower
+    // from 2^21)
+    const int team_req = p ? p->team : 0;
+    const bool one = team_req == 5 || (team_req == 0 && !P->sorted && k <= (n >> 11));
+    P->one_cta = (one && fused_one_ready(di->device, P->km, smem)) ? 1 : 0;
   }
   // team of the phases after the sampler: one CTA with the sets in shared
   // memory when they are small (their cost is then round trips, not
