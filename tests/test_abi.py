@@ -87,3 +87,28 @@ def test_autotune_choices_are_valid():
 
 def test_cli_binary_built():
     assert os.path.exists(os.path.join(os.path.dirname(D.LIB_PATH), "topk.bin"))
+
+
+def test_autotune_small_problem_and_float_rules():
+    # up to 2^13 keys the plain select fits one CTA; up to 2^16 keys it stays
+    # the choice above k = 64
+    assert D.autotune(1 << 13, 5).algo == D.ALGO_PLAIN_RADIX
+    assert D.autotune(1 << 16, 128).algo == D.ALGO_PLAIN_RADIX
+    p = D.autotune(1 << 16, 16)
+    assert p.algo != D.ALGO_PLAIN_RADIX and p.path in (1, 2)
+    # small k: the delegate vector is kept small enough for the one-CTA tail
+    for log2n, k in [(20, 1), (20, 128), (22, 1), (22, 16)]:
+        p = D.autotune(1 << log2n, k)
+        m = (1 << log2n) >> p.alpha
+        assert p.path in (1, 2) and (m if p.path == 1 else 2 * m) <= 8192, (log2n, k, p.path, p.alpha)
+    # float keys from 2^22: delegate paths below k = 2^13, the sampled threshold from there
+    for k in (1, 16, 256, 4096):
+        assert D.autotune(1 << 28, k, D.F32).path in (1, 2), k
+    for k in (1 << 13, 1 << 16, 1 << 20):
+        assert D.autotune(1 << 28, k, D.F32).path == 4, k
+    # the N = 2^30 uint32 choices: beta path (alpha 11, 10 from k = 2^15), sampled threshold from 2^17
+    for k, alpha in ((1, 11), (1 << 10, 11), (1 << 16, 10)):
+        p = D.autotune(1 << 30, k)
+        assert (p.path, p.alpha) == (2, alpha), (k, p.path, p.alpha)
+    for k in (1 << 17, 1 << 24):
+        assert D.autotune(1 << 30, k).path == 4
