@@ -122,3 +122,13 @@ def test_heavy_ties_and_constant_input():
         for k in (1, 1000, x.size // 2, x.size):
             check(x, k)
             check(x, k, sorted=False)
+
+
+def test_last_levels_team_follows_k():
+    # unsorted selects with k <= n/2048 finish their last levels in one CTA,
+    # larger ones and sorted outputs on the cooperative grid
+    x = O.gen("u32", 1 << 22, 99)
+    assert check(x, 1 << 11, sorted=False)["team_cluster"] == 5
+    assert check(x, 1 << 11, largest=False, sorted=False)["team_cluster"] == 5
+    assert check(x, (1 << 11) + 1, sorted=False)["team_cluster"] == 0
+    assert check(x, 1 << 11, sorted=True)["team_cluster"] == 0
